@@ -1,0 +1,140 @@
+/*
+ * sgs_b200.h - C ABI of the B200 stochastic Gaussian splatting render path.
+ *
+ * One call renders one stochastic sample ("sample-frame") of a 3D Gaussian splatting scene and
+ * merges it into the caller's progressive history, exactly like one `_C.render(...)` call of the
+ * reference extension StochasticGSCudaBackend (StochasticGSCudaBackend/render.cu:16-158, bound by
+ * PYBIND11_MODULE at render.cu:162-165 and wrapped by StochasticGSCudaBackend/render.py:72-96).
+ * Plain pointers and sizes only: every array pointer is a device pointer of the current CUDA
+ * device, row-major and contiguous, and `stream` is a cudaStream_t (NULL = legacy default stream).
+ * Calls are asynchronous with respect to the host; the functions never synchronise the device.
+ *
+ * Status codes: 0 success, negative on error; sgs_last_error() describes the last error of the
+ * calling thread. Invalid arguments are rejected before any launch (the reference does not
+ * validate and traps on an invalid temporal mode, resolve.cu:342).
+ */
+#ifndef SGS_B200_H
+#define SGS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGS_ABI_VERSION 1
+#define SGS_K_BUFFER_SIZE 4 /* k-buffer entries per (sub)pixel, resolve.h:9 / render.cu:164 */
+
+enum sgs_status {
+    SGS_OK = 0,
+    SGS_ERROR_INVALID_ARGUMENT = -1,
+    SGS_ERROR_WORKSPACE = -2, /* workspace missing, misaligned or smaller than sgs_workspace_size() */
+    SGS_ERROR_CUDA = -3       /* a CUDA runtime call or launch failed */
+};
+
+enum sgs_temporal_mode { /* StochasticGSCudaBackend/render.py:44-47, resolve.h:11-15 */
+    SGS_TEMPORAL_RESET = 0,
+    SGS_TEMPORAL_STATIC = 1,
+    SGS_TEMPORAL_REPROJECT = 2
+};
+
+/* Gaussian model in the layout of Model.py:22-79 (render.cu:17-21). */
+typedef struct sgs_gaussians {
+    const float* means;           /* (N, 3) world positions */
+    const float* scales;          /* (N, 3) log scales */
+    const float* rotations;       /* (N, 4) quaternions (r, i, j, k), any norm; 16-byte aligned */
+    const float* opacities;       /* (N) opacity logits */
+    const float* sh_coefficients; /* (N, B, 3) SH coefficients */
+    uint32_t n_gaussians;         /* N (0 renders background) */
+    uint32_t sh_bases;            /* B: 1, 4, 9 or 16 (degree 0..3) */
+} sgs_gaussians;
+
+/* Pinhole camera in image pixels (render.cu:22-31, render_utils.h:19-30). */
+typedef struct sgs_camera {
+    const float* w2c;          /* world-to-view, >= 3 rows of 4 floats; 16-byte aligned */
+    const float* cam_position; /* (3) camera position in world space */
+    uint32_t width;            /* image width in pixels */
+    uint32_t height;           /* image height in pixels */
+    float focal_x, focal_y;    /* focal lengths in pixels */
+    float center_x, center_y;  /* principal point in pixels (x right, y down) */
+    float near_plane, far_plane;
+} sgs_camera;
+
+/* Switches of one call (render.cu:32-37,44-45). */
+typedef struct sgs_settings {
+    int32_t proper_antialiasing;
+    int32_t supersampling_factor;            /* values < 1 act as 1 (render.cu:52) */
+    int32_t use_gps;                         /* Gaussian point splatting instead of stochastic transparency */
+    int32_t hybrid_scheduling;               /* load-balanced pass for large Gaussians */
+    int32_t spatial_reuse;                   /* resample the four neighbours through the k-buffer */
+    int32_t temporal_mode;                   /* enum sgs_temporal_mode */
+    const uint8_t* blue_noise;               /* (64, 128, 128) u8 volume, or NULL for white noise */
+    const float* view_to_previous_view;      /* 4x4 row-major, read in REPROJECT mode; 16-byte aligned */
+    uint32_t max_fragments;                  /* GPS points per Gaussian cap; 0 = W*H/2 as the reference */
+    uint32_t max_binned;                     /* hybrid GPS bin capacity; 0 = min(N, 2^20) as the reference */
+} sgs_settings;
+
+/* Caller-owned state carried between calls (render.cu:38-43). */
+typedef struct sgs_history {
+    const float* image;        /* (H, W, 3) previous premultiplied colour; read in STATIC / REPROJECT */
+    const float* depth;        /* (H, W, 1) */
+    const float* alpha;        /* (H, W, 1) */
+    const float* weight_mass;  /* (H, W, 1) */
+    int32_t* k_buffer_primitives; /* (K, P_fb, 2) (index, depth bits); updated in place with spatial reuse */
+    float* k_buffer_occlusion;    /* (K, P_fb, 4); updated in place with spatial reuse */
+} sgs_history;
+
+/* Freshly written outputs (render.cu:59-62), the next call's history. May not alias the history. */
+typedef struct sgs_outputs {
+    float* image;       /* (H, W, 3) colour premultiplied by alpha */
+    float* depth;       /* (H, W, 1) depth premultiplied by alpha */
+    float* alpha;       /* (H, W, 1) */
+    float* weight_mass; /* (H, W, 1) accumulated resampling weight */
+} sgs_outputs;
+
+/* Offsets (bytes, from the workspace start) of the intermediate buffers of sgs_render. */
+typedef struct sgs_workspace_layout {
+    size_t framebuffer;   /* uint64 (P_fb): packed (depth_bits << 32 | index) winners, ~0 = empty */
+    size_t samples;       /* float (P_fb, 4): winner colour and depth (0 = background) */
+    size_t reuse_weights; /* float (P_fb, 4) with spatial reuse, else unused */
+    size_t queue;         /* large-Gaussian work queue */
+    size_t total;         /* == sgs_workspace_size() */
+} sgs_workspace_layout;
+
+/* Scratch bytes sgs_render needs for these arguments (replaces the per-call allocations of
+ * render.cu:63-65, accumulate_hybrid.cu:356-366 and accumulate_hybrid_gps.cu:212-219). The
+ * workspace must be 256-byte aligned; it need not be initialised. */
+size_t sgs_workspace_size(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings);
+
+/* Fills `layout` for these arguments; returns SGS_OK or an error status. */
+int sgs_get_workspace_layout(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                             sgs_workspace_layout* layout);
+
+/* One sample-frame (replaces `_C.render`, render.cu:16-158): clears the framebuffer, accumulates
+ * the closest accepted fragment per (sub)pixel, evaluates the winners' colours, resolves and
+ * merges with the history. Uses and then increments the process-wide frame index, which seeds
+ * every random number (render.cu:56-57). Enqueued on `stream`; no host synchronisation. */
+int sgs_render(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+               const sgs_history* history, const sgs_outputs* outputs, void* workspace, size_t workspace_bytes,
+               void* stream);
+
+/* Process-wide frame index (render.cu:56-57 keeps it in a hidden static counter that starts at 0);
+ * exposed so that random streams can be pinned and resumed. */
+uint32_t sgs_get_frame_index(void);
+void sgs_set_frame_index(uint32_t frame_index);
+
+/* K of the k-buffer (render.cu:164, `_C.k_buffer_size`). */
+uint32_t sgs_k_buffer_size(void);
+
+/* ABI version of the loaded library (SGS_ABI_VERSION). */
+int sgs_abi_version(void);
+
+/* Human-readable description of the calling thread's last error ("" when none). */
+const char* sgs_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGS_B200_H */

@@ -1,0 +1,176 @@
+"""Drop-in replacement of the reference extension module `StochasticGSCudaBackend._C`.
+
+`render(...)` takes the same 29 positional arguments as the reference binding
+(StochasticGSCudaBackend/render.cu:16-45, bound at render.cu:162-165) and returns the same tuple of
+four freshly allocated CUDA tensors (image, depth, alpha, weight_mass). It validates the inputs,
+allocates the outputs and a scratch workspace through PyTorch's caching allocator on the inputs'
+device, and calls the C ABI (include/sgs_b200.h) on the current PyTorch stream. All compute runs in
+the CUDA kernels of libsgs_b200.so; there is no CPU path.
+
+Extras beyond the reference module: `get_frame_index` / `set_frame_index` expose the process-wide
+frame counter that seeds the random numbers (a hidden static in render.cu:56-57), and
+`render_with_workspace` additionally returns the scratch workspace and its layout so callers can
+inspect the winner framebuffer and the samples.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _abi
+
+_lib = _abi.load()
+
+k_buffer_size: int = int(_lib.sgs_k_buffer_size())
+
+_VALID_SH_BASES = (1, 4, 9, 16)
+
+
+def get_frame_index() -> int:
+    return int(_lib.sgs_get_frame_index())
+
+
+def set_frame_index(frame_index: int) -> None:
+    _lib.sgs_set_frame_index(int(frame_index) & 0xFFFFFFFF)
+
+
+def _check(cond: bool, msg: str) -> None:
+    if not cond:
+        raise RuntimeError(msg)
+
+
+def _cuda_f32(t: torch.Tensor, name: str, device: torch.device) -> torch.Tensor:
+    _check(isinstance(t, torch.Tensor), f"{name} must be a tensor")
+    _check(t.is_cuda and t.device == device, f"{name} must be a CUDA tensor on {device}")
+    _check(t.dtype == torch.float32, f"{name} must be float32")
+    return t.contiguous()
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None or t.numel() == 0 else t.data_ptr()
+
+
+def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, width, height, focal_x, focal_y,
+             center_x, center_y, near_plane, far_plane, proper_antialiasing, supersampling_factor_raw, use_gps,
+             hybrid_scheduling, spatial_reuse, blue_noise, k_buffer_primitives, k_buffer_occlusion, history_image,
+             history_depth, history_alpha, history_weight_mass, view_to_previous_view, temporal_mode):
+    _check(isinstance(means, torch.Tensor) and means.is_cuda, "means must be a CUDA tensor")
+    device = means.device
+    means = _cuda_f32(means, "means", device)
+    n = means.shape[0]
+    _check(means.dim() == 2 and means.shape[1] == 3, "means must have shape (N, 3)")
+    scales = _cuda_f32(scales, "scales", device)
+    _check(tuple(scales.shape) == (n, 3), "scales must have shape (N, 3)")
+    rotations = _cuda_f32(rotations, "rotations", device)
+    _check(tuple(rotations.shape) == (n, 4), "rotations must have shape (N, 4)")
+    opacities = _cuda_f32(opacities, "opacities", device)
+    _check(opacities.numel() == n, "opacities must hold N values")
+    sh_coefficients = _cuda_f32(sh_coefficients, "sh_coefficients", device)
+    _check(sh_coefficients.dim() == 3 and sh_coefficients.shape[0] == n and sh_coefficients.shape[2] == 3,
+           "sh_coefficients must have shape (N, B, 3)")
+    sh_bases = sh_coefficients.shape[1]
+    _check(sh_bases in _VALID_SH_BASES, f"sh_coefficients must have 1, 4, 9 or 16 bases, got {sh_bases}")
+    w2c = _cuda_f32(w2c, "w2c", device)
+    _check(w2c.numel() >= 12 and w2c.shape[-1] == 4, "w2c must hold at least 3 rows of 4 floats")
+    cam_position = _cuda_f32(cam_position, "cam_position", device)
+    _check(cam_position.numel() == 3, "cam_position must hold 3 floats")
+    width, height = int(width), int(height)
+    _check(0 < width < 2 ** 32 and 0 < height < 2 ** 32, "width and height must be positive")
+    ss = max(1, int(supersampling_factor_raw))
+    n_fb = width * height * ss * ss
+    n_px = width * height
+    mode = int(temporal_mode)
+    _check(mode in (0, 1, 2), f"invalid temporal mode {mode}")
+
+    if blue_noise is not None and blue_noise.numel() > 0:
+        _check(blue_noise.is_cuda and blue_noise.device == device and blue_noise.dtype == torch.uint8
+               and blue_noise.numel() == 64 * 128 * 128, "blue_noise must be a (64, 128, 128) uint8 CUDA tensor")
+        blue_noise = blue_noise.contiguous()
+    else:
+        blue_noise = None
+
+    if spatial_reuse:
+        k = k_buffer_size
+        _check(k_buffer_primitives.is_cuda and k_buffer_primitives.device == device
+               and k_buffer_primitives.dtype == torch.int32 and tuple(k_buffer_primitives.shape) == (k, n_fb, 2)
+               and k_buffer_primitives.is_contiguous(), f"k_buffer_primitives must be a contiguous ({k}, {n_fb}, 2) int32 CUDA tensor")
+        _check(k_buffer_occlusion.is_cuda and k_buffer_occlusion.device == device
+               and k_buffer_occlusion.dtype == torch.float32 and tuple(k_buffer_occlusion.shape) == (k, n_fb, 4)
+               and k_buffer_occlusion.is_contiguous(), f"k_buffer_occlusion must be a contiguous ({k}, {n_fb}, 4) float32 CUDA tensor")
+
+    if mode != 0:
+        for name, t, ch in (("history_image", history_image, 3), ("history_depth", history_depth, 1),
+                            ("history_alpha", history_alpha, 1), ("history_weight_mass", history_weight_mass, 1)):
+            _check(isinstance(t, torch.Tensor) and t.is_cuda and t.device == device and t.dtype == torch.float32
+                   and t.numel() == n_px * ch and t.is_contiguous(),
+                   f"{name} must be a contiguous ({height}, {width}, {ch}) float32 CUDA tensor in temporal mode {mode}")
+    if mode == 2:
+        view_to_previous_view = _cuda_f32(view_to_previous_view, "view_to_previous_view", device)
+        _check(view_to_previous_view.numel() >= 12, "view_to_previous_view must be a 4x4 matrix")
+    else:
+        view_to_previous_view = None
+
+    g = _abi.Gaussians(_ptr(means), _ptr(scales), _ptr(rotations), _ptr(opacities), _ptr(sh_coefficients), n, sh_bases)
+    c = _abi.Camera(w2c.data_ptr(), cam_position.data_ptr(), width, height, float(focal_x), float(focal_y),
+                    float(center_x), float(center_y), float(near_plane), float(far_plane))
+    s = _abi.SettingsC(int(bool(proper_antialiasing)), ss, int(bool(use_gps)), int(bool(hybrid_scheduling)),
+                       int(bool(spatial_reuse)), mode, _ptr(blue_noise), _ptr(view_to_previous_view), 0, 0)
+    h = _abi.HistoryC(
+        _ptr(history_image) if mode else None, _ptr(history_depth) if mode else None,
+        _ptr(history_alpha) if mode else None, _ptr(history_weight_mass) if mode else None,
+        _ptr(k_buffer_primitives) if spatial_reuse else None, _ptr(k_buffer_occlusion) if spatial_reuse else None)
+    # keep the contiguous copies alive for the duration of the call
+    keep = (means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, blue_noise, view_to_previous_view)
+    return device, g, c, s, h, (width, height), keep
+
+
+def _render_impl(args, want_workspace: bool):
+    device, g, c, s, h, (width, height), keep = _prepare(*args)
+    with torch.cuda.device(device):
+        opts = dict(dtype=torch.float32, device=device)
+        image = torch.empty((height, width, 3), **opts)
+        depth = torch.empty((height, width, 1), **opts)
+        alpha = torch.empty((height, width, 1), **opts)
+        weight_mass = torch.empty((height, width, 1), **opts)
+        o = _abi.Outputs(image.data_ptr(), depth.data_ptr(), alpha.data_ptr(), weight_mass.data_ptr())
+        ws_bytes = int(_lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s)))
+        if ws_bytes == 0:
+            raise RuntimeError(_abi.last_error(_lib) or "invalid render arguments")
+        workspace = torch.empty((ws_bytes,), dtype=torch.uint8, device=device)
+        stream = torch.cuda.current_stream(device).cuda_stream
+        status = _lib.sgs_render(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h), ctypes.byref(o),
+                                 ctypes.c_void_p(workspace.data_ptr()), ctypes.c_size_t(ws_bytes),
+                                 ctypes.c_void_p(stream))
+        if status != _abi.SGS_OK:
+            raise RuntimeError(f"sgs_render failed ({status}): {_abi.last_error(_lib)}")
+        del keep
+        if not want_workspace:
+            return image, depth, alpha, weight_mass
+        layout = _abi.WorkspaceLayout()
+        _lib.sgs_get_workspace_layout(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(layout))
+        return (image, depth, alpha, weight_mass), workspace, layout
+
+
+def render(*args):
+    """`_C.render` with the reference's 29 positional arguments; returns (image, depth, alpha, weight_mass)."""
+    if len(args) != 29:
+        raise TypeError(f"render() takes 29 positional arguments ({len(args)} given)")
+    return _render_impl(args, want_workspace=False)
+
+
+def render_with_workspace(*args):
+    """As `render`, plus the workspace tensor and its layout (winner framebuffer, samples, reuse weights)."""
+    if len(args) != 29:
+        raise TypeError(f"render_with_workspace() takes 29 positional arguments ({len(args)} given)")
+    return _render_impl(args, want_workspace=True)
+
+
+def workspace_views(workspace: torch.Tensor, layout, n_fb: int, spatial_reuse: bool) -> dict[str, torch.Tensor]:
+    """Typed views of a workspace returned by `render_with_workspace`."""
+    fb = workspace[layout.framebuffer:layout.framebuffer + 8 * n_fb].view(torch.int64)
+    samples = workspace[layout.samples:layout.samples + 16 * n_fb].view(torch.float32).view(n_fb, 4)
+    out = {"framebuffer": fb, "samples": samples}
+    if spatial_reuse:
+        out["reuse_weights"] = workspace[layout.reuse_weights:layout.reuse_weights + 16 * n_fb].view(torch.float32).view(n_fb, 4)
+    return out

@@ -1,0 +1,137 @@
+"""ctypes declaration of the C ABI in include/sgs_b200.h and the loader of libsgs_b200.so.
+
+The library is required: importing this module raises if it is missing or was built for another
+ABI version. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_NAME = "libsgs_b200.so"
+ABI_VERSION = 1
+
+SGS_OK = 0
+SGS_ERROR_INVALID_ARGUMENT = -1
+SGS_ERROR_WORKSPACE = -2
+SGS_ERROR_CUDA = -3
+
+
+class Gaussians(ctypes.Structure):
+    _fields_ = [
+        ("means", ctypes.c_void_p),
+        ("scales", ctypes.c_void_p),
+        ("rotations", ctypes.c_void_p),
+        ("opacities", ctypes.c_void_p),
+        ("sh_coefficients", ctypes.c_void_p),
+        ("n_gaussians", ctypes.c_uint32),
+        ("sh_bases", ctypes.c_uint32),
+    ]
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [
+        ("w2c", ctypes.c_void_p),
+        ("cam_position", ctypes.c_void_p),
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("focal_x", ctypes.c_float),
+        ("focal_y", ctypes.c_float),
+        ("center_x", ctypes.c_float),
+        ("center_y", ctypes.c_float),
+        ("near_plane", ctypes.c_float),
+        ("far_plane", ctypes.c_float),
+    ]
+
+
+class SettingsC(ctypes.Structure):
+    _fields_ = [
+        ("proper_antialiasing", ctypes.c_int32),
+        ("supersampling_factor", ctypes.c_int32),
+        ("use_gps", ctypes.c_int32),
+        ("hybrid_scheduling", ctypes.c_int32),
+        ("spatial_reuse", ctypes.c_int32),
+        ("temporal_mode", ctypes.c_int32),
+        ("blue_noise", ctypes.c_void_p),
+        ("view_to_previous_view", ctypes.c_void_p),
+        ("max_fragments", ctypes.c_uint32),
+        ("max_binned", ctypes.c_uint32),
+    ]
+
+
+class HistoryC(ctypes.Structure):
+    _fields_ = [
+        ("image", ctypes.c_void_p),
+        ("depth", ctypes.c_void_p),
+        ("alpha", ctypes.c_void_p),
+        ("weight_mass", ctypes.c_void_p),
+        ("k_buffer_primitives", ctypes.c_void_p),
+        ("k_buffer_occlusion", ctypes.c_void_p),
+    ]
+
+
+class Outputs(ctypes.Structure):
+    _fields_ = [
+        ("image", ctypes.c_void_p),
+        ("depth", ctypes.c_void_p),
+        ("alpha", ctypes.c_void_p),
+        ("weight_mass", ctypes.c_void_p),
+    ]
+
+
+class WorkspaceLayout(ctypes.Structure):
+    _fields_ = [
+        ("framebuffer", ctypes.c_size_t),
+        ("samples", ctypes.c_size_t),
+        ("reuse_weights", ctypes.c_size_t),
+        ("queue", ctypes.c_size_t),
+        ("total", ctypes.c_size_t),
+    ]
+
+
+# every entry point of include/sgs_b200.h: name -> (restype, argtypes)
+SIGNATURES = {
+    "sgs_workspace_size": (ctypes.c_size_t, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC)]),
+    "sgs_get_workspace_layout": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
+                                                ctypes.POINTER(SettingsC), ctypes.POINTER(WorkspaceLayout)]),
+    "sgs_render": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC),
+                                  ctypes.POINTER(HistoryC), ctypes.POINTER(Outputs), ctypes.c_void_p, ctypes.c_size_t,
+                                  ctypes.c_void_p]),
+    "sgs_get_frame_index": (ctypes.c_uint32, []),
+    "sgs_set_frame_index": (None, [ctypes.c_uint32]),
+    "sgs_k_buffer_size": (ctypes.c_uint32, []),
+    "sgs_abi_version": (ctypes.c_int, []),
+    "sgs_last_error": (ctypes.c_char_p, []),
+}
+
+
+def library_path() -> Path:
+    return Path(__file__).resolve().parent / LIB_NAME
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the library once and declares every entry point; raises when it is unusable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not path.is_file():
+        raise ImportError(f"{path} is missing: build it with `python stochastic-gaussian-splatting_b200/build.py`")
+    lib = ctypes.CDLL(str(path))
+    for name, (restype, argtypes) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    version = lib.sgs_abi_version()
+    if version != ABI_VERSION:
+        raise ImportError(f"{path} has ABI version {version}, expected {ABI_VERSION}")
+    _lib = lib
+    return lib
+
+
+def last_error(lib: ctypes.CDLL) -> str:
+    msg = lib.sgs_last_error()
+    return msg.decode() if msg else ""

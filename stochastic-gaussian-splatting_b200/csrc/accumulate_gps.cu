@@ -1,0 +1,212 @@
+// Gaussian point splatting accumulation (USE_GPS), scatter and hybrid scheduling.
+//
+// Follows accumulate_scatter.cu:79-146, scatter_utils.cuh:98-183 and accumulate_hybrid_gps.cu:27-181.
+// Each Gaussian emits min(Poisson(2 pi sqrt(det) dilog(opacity)), cap) points drawn from its
+// opacity-truncated 2-D distribution; a point that lands in the framebuffer and whose pixel
+// centre lies inside the alpha threshold merges the Gaussian's key with a u64 atomicMin.
+//
+// The scatter path's random numbers are a per-lane stream: lane l of the warp that owns
+// Gaussians [32w, 32w + 32) draws from seed(32w + l) for its own first <= 4 points and then,
+// in the cooperative phase, for every point it evaluates of the warp's larger Gaussians, in lane
+// order. The winners therefore depend on that exact warp grouping and draw order, and this
+// kernel keeps both (culled and padding lanes still draw their Poisson sample).
+//
+// Hybrid scheduling bins the Gaussians with more than 512 points (up to max_binned of them) into
+// the device-side work queue; their points use counter-based seeds (seed ^ point * golden
+// ratio), so the queue's persistent consumer may process their 256-point chunks in any order.
+// Unlike the reference there is no host synchronisation between the passes.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "sgs_internal.h"
+
+namespace sgs {
+namespace {
+
+constexpr uint32_t kBlock = 256;
+constexpr uint32_t kFullMask = 0xffffffffu;
+constexpr uint32_t kBinningPointThreshold = 512;  // accumulate_hybrid_gps.cu:21
+constexpr uint32_t kChunkPoints = 256;             // accumulate_hybrid_gps.cu:19
+constexpr uint32_t kQueueBlocksPerSM = 8;
+
+struct PointSource {
+    float2 mean2d;
+    float3 conic;
+    float3 L;  // Cholesky factor of the 2-D covariance: (l11, l21, l22)
+    float power_threshold;
+    float opacity_rcp;
+    float opacity_dilog;
+    unsigned long long key;
+};
+
+// Draws one point from `seed` and merges it (scatter_utils.cuh:116-129).
+__device__ __forceinline__ void gps_point(const AccumulateParams& a, uint2& seed, const PointSource& s) {
+    const float2 u = pcg2d_uniform(seed);
+    const float2 xy = truncated_box_muller(u.x, u.y, s.opacity_rcp, s.opacity_dilog);
+    const float sx = s.mean2d.x + s.L.x * xy.x;
+    const float sy = s.mean2d.y + (s.L.y * xy.x + s.L.z * xy.y);
+    if (sx >= a.cam.width || sx < 0.0f || sy >= a.cam.height || sy < 0.0f) return;
+    const float dcx = truncf(sx) + 0.5f - s.mean2d.x;
+    const float dcy = truncf(sy) + 0.5f - s.mean2d.y;
+    const float power = 0.5f * (s.conic.x * dcx * dcx + s.conic.z * dcy * dcy) + s.conic.y * dcx * dcy;
+    if (power > s.power_threshold) return;
+    const uint32_t px = __float2uint_rd(sx);
+    const uint32_t py = __float2uint_rd(sy);
+    atomicMin(&a.framebuffer[py * a.cam.width_int + px], s.key);
+}
+
+__device__ __forceinline__ PointSource shfl_source(const PointSource& s, const uint32_t src) {
+    PointSource o;
+    o.mean2d = make_float2(__shfl_sync(kFullMask, s.mean2d.x, src), __shfl_sync(kFullMask, s.mean2d.y, src));
+    o.conic = make_float3(__shfl_sync(kFullMask, s.conic.x, src), __shfl_sync(kFullMask, s.conic.y, src),
+                          __shfl_sync(kFullMask, s.conic.z, src));
+    o.L = make_float3(__shfl_sync(kFullMask, s.L.x, src), __shfl_sync(kFullMask, s.L.y, src),
+                      __shfl_sync(kFullMask, s.L.z, src));
+    o.power_threshold = __shfl_sync(kFullMask, s.power_threshold, src);
+    o.opacity_rcp = __shfl_sync(kFullMask, s.opacity_rcp, src);
+    o.opacity_dilog = __shfl_sync(kFullMask, s.opacity_dilog, src);
+    o.key = __shfl_sync(kFullMask, s.key, src);
+    return o;
+}
+
+__global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulateParams a) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
+    bool active = idx < a.n;
+    const uint32_t g = active ? idx : a.n - 1;
+
+    Projected p;
+    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p)) return;
+
+    // importance and number of points (accumulate_scatter.cu:104-112)
+    PointSource s;
+    s.opacity_dilog = gps_dilog(p.opacity);
+    const float importance = kTwoPi * sqrtf(p.determinant) * s.opacity_dilog;
+    uint2 seed = gps_seed(g, a.frame_idx);
+    const uint32_t true_count = poisson_count(seed, importance);
+    if (true_count == 0) active = false;
+    const uint32_t cap = a.max_fragments != 0
+                             ? a.max_fragments
+                             : __float2uint_rn(a.cam.width * a.cam.height / (2.0f * a.cam.ss * a.cam.ss));
+    const uint32_t count = min(true_count, cap);
+    if (__ballot_sync(kFullMask, active) == 0) return;
+
+    const float c0 = sqrtf(p.cov2d.x);
+    const float c1 = p.cov2d.y / c0;
+    const float c2 = sqrtf(p.cov2d.z - c1 * c1);
+    s.mean2d = p.mean2d;
+    s.conic = p.conic;
+    s.L = make_float3(c0, c1, c2);
+    s.power_threshold = p.power_threshold;
+    s.opacity_rcp = 1.0f / fmaxf(p.opacity, 1.0e-37f);
+    s.key = pack_fragment(p.depth, g);
+
+    if (a.hybrid) {
+        // bin Gaussians with many points: one 64-bit atomic per warp reserves entries and chunks
+        const bool want = active && count > kBinningPointThreshold;
+        const uint32_t ballot = __ballot_sync(kFullMask, want);
+        if (ballot != 0) {
+            const uint32_t chunks = want ? (count + kChunkPoints - 1) / kChunkPoints : 0u;
+            uint32_t incl = chunks;
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(kFullMask, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t warp_chunks = __shfl_sync(kFullMask, incl, 31);
+            const uint32_t leader = __ffs(ballot) - 1;
+            unsigned long long base = 0;
+            if (lane == leader)
+                base = atomicAdd(&a.queue->packed,
+                                 (static_cast<unsigned long long>(__popc(ballot)) << kQueueEntryShift) | warp_chunks);
+            base = __shfl_sync(kFullMask, base, leader);
+            const uint32_t e = static_cast<uint32_t>(base >> kQueueEntryShift) + __popc(ballot & ((1u << lane) - 1u));
+            const unsigned long long first_chunk = (base & kQueueChunkMask) + (incl - chunks);
+            if (want && e < a.max_binned && e < a.q.capacity && first_chunk + chunks <= 0xffffffffull) {
+                a.q.key[e] = s.key;
+                a.q.geom[e] = make_float4(s.mean2d.x, s.mean2d.y, s.L.x, s.L.y);
+                a.q.geom2[e] = make_float4(s.L.z, s.power_threshold, s.opacity_rcp, s.opacity_dilog);
+                a.q.meta[e] = make_uint4(__float_as_uint(s.conic.x), __float_as_uint(s.conic.y),
+                                         __float_as_uint(s.conic.z), static_cast<uint32_t>(first_chunk));
+                a.q.count[e] = count;
+                active = false;
+            }
+        }
+    }
+
+    // own first points, sequentially per lane
+    for (uint32_t i = 0; active && i < count && i < kSequentialFragments; ++i) gps_point(a, seed, s);
+
+    // the rest cooperatively, one large Gaussian at a time in lane order, each lane on its own seed
+    const uint32_t coop = __ballot_sync(kFullMask, active && count > kSequentialFragments);
+    uint32_t pending = coop;
+    while (pending) {
+        const uint32_t src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint32_t n_src = __shfl_sync(kFullMask, count, src);
+        const PointSource t = shfl_source(s, src);
+        const uint32_t iterations = (n_src - kSequentialFragments + 31) / 32;
+        for (uint32_t it = 0; it < iterations; ++it) {
+            const uint32_t fi = it * 32 + lane + kSequentialFragments;
+            if (fi >= n_src) continue;
+            gps_point(a, seed, t);
+        }
+    }
+}
+
+// Persistent consumer of the binned Gaussians: each warp steals one 256-point chunk at a time
+// (accumulate_hybrid_gps.cu:126-181 with per-point counter-based seeds).
+__global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParams a) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned long long packed = a.queue->packed;
+    const uint32_t cap = min(a.max_binned, a.q.capacity);
+    const uint32_t n_entries = static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(cap)));
+    if (n_entries == 0) return;
+    const uint32_t last_first = a.q.meta[n_entries - 1].w;
+    const uint32_t n_chunks = last_first + (a.q.count[n_entries - 1] + kChunkPoints - 1) / kChunkPoints;
+    for (;;) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(&a.queue->next_chunk, 1u);
+        c = __shfl_sync(kFullMask, c, 0);
+        if (c >= n_chunks) break;
+        uint32_t lo = 0, hi = n_entries - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (a.q.meta[mid].w <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const uint4 m = a.q.meta[lo];
+        const float4 gm = a.q.geom[lo];
+        const float4 gm2 = a.q.geom2[lo];
+        PointSource s;
+        s.key = a.q.key[lo];
+        s.mean2d = make_float2(gm.x, gm.y);
+        s.L = make_float3(gm.z, gm.w, gm2.x);
+        s.power_threshold = gm2.y;
+        s.opacity_rcp = gm2.z;
+        s.opacity_dilog = gm2.w;
+        s.conic = make_float3(__uint_as_float(m.x), __uint_as_float(m.y), __uint_as_float(m.z));
+        const uint32_t n_points = a.q.count[lo];
+        const uint32_t gaussian = static_cast<uint32_t>(s.key);
+        const uint2 base_seed = gps_seed(gaussian, a.frame_idx);
+        const uint32_t first_point = (c - m.w) * kChunkPoints;
+        for (uint32_t k = lane; k < kChunkPoints; k += 32) {
+            const uint32_t point = first_point + k;
+            if (point >= n_points) break;
+            uint2 seed = base_seed;
+            seed.x ^= point * 0x9E3779B9u;
+            gps_point(a, seed, s);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_accumulate_gps(const AccumulateParams& p, const int num_sms, cudaStream_t stream) {
+    if (p.n == 0) return cudaSuccess;
+    const unsigned grid = (p.n + kBlock - 1) / kBlock;
+    gps_scatter_kernel<<<grid, kBlock, 0, stream>>>(p);
+    if (p.hybrid) gps_queue_kernel<<<static_cast<unsigned>(num_sms) * kQueueBlocksPerSM, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace sgs

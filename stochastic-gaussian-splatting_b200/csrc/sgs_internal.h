@@ -1,0 +1,101 @@
+// Internal host-side interface between the C ABI (render_abi.cu) and the kernel files.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "sgs_project.cuh"
+
+namespace sgs {
+
+// Large-Gaussian work queue shared by the ST and GPS accumulate passes. Entries are appended
+// with one 64-bit atomicAdd on `packed` = (entry count << 40) | chunk count, so every entry's
+// first chunk index is known at insertion and increases with the entry index.
+struct WorkQueue {
+    unsigned long long packed;   // (entries << 40) | chunks, reserved by producers
+    unsigned int next_chunk;     // work-stealing cursor of the consumer kernel
+    unsigned int overflow;       // producers that found the queue full (processed in place)
+    unsigned int error;          // nonzero when a consumer met an inconsistent entry
+    unsigned int pad[3];
+};
+constexpr unsigned long long kQueueEntryShift = 40;
+constexpr unsigned long long kQueueChunkMask = (1ull << kQueueEntryShift) - 1;
+
+// Per-entry arrays of the large-Gaussian queue (structure of arrays, 16-byte aligned).
+struct QueueArrays {
+    unsigned long long* key;  // packed fragment key
+    float4* geom;             // ST: mean2d - 0.5 (x, y), exp2-scaled conic (x, y); GPS: mean2d, L.x, L.y
+    float4* geom2;            // ST: conic z, opacity, x_min, width (bit casts); GPS: L.z, power threshold, opacity_rcp, dilog
+    uint4* meta;              // ST: y_min, height, rows per chunk, first chunk; GPS: conic x/y/z bits, first chunk
+    uint32_t* count;          // GPS: number of points
+    uint32_t capacity;
+};
+
+// Scratch carved out of the caller's workspace by layout_workspace().
+struct Workspace {
+    unsigned long long* framebuffer;  // P_fb packed keys
+    float4* samples;                  // P_fb (rgb, depth)
+    float4* reuse_weights;            // P_fb when spatial reuse is on
+    WorkQueue* queue;
+    QueueArrays q;
+    size_t bytes;
+};
+
+struct AccumulateParams {
+    const float* means;
+    const float* scales;
+    const float4* rotations;
+    const float* opacities;
+    const float4* w2c;
+    unsigned long long* framebuffer;
+    uint32_t n;
+    uint32_t frame_idx;
+    PassCamera cam;
+    const uint8_t* blue_noise_slice;  // null: white noise
+    uint32_t blue_noise_rotation;
+    uint32_t max_fragments;           // GPS point cap per Gaussian
+    uint32_t max_binned;              // hybrid GPS: binned Gaussian capacity
+    bool hybrid;                      // hybrid scheduling
+    WorkQueue* queue;
+    QueueArrays q;
+};
+
+cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue* queue, cudaStream_t stream);
+cudaError_t launch_accumulate_st(const AccumulateParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_accumulate_gps(const AccumulateParams& p, int num_sms, cudaStream_t stream);
+
+struct ResolveParams {
+    const float* means;
+    const float* scales;
+    const float4* rotations;
+    const float* opacities;
+    const float* sh;
+    const float4* w2c;
+    const float* cam_position;
+    const unsigned long long* framebuffer;
+    float4* samples;
+    float4* reuse_weights;
+    uint2* k_prims;
+    float4* k_occl;
+    const float* hist_image;
+    const float* hist_depth;
+    const float* hist_alpha;
+    const float* hist_weight_mass;
+    const float4* v2pv;
+    float* image;
+    float* depth;
+    float* alpha;
+    float* weight_mass;
+    uint32_t n_fb;
+    uint32_t n_pixels;
+    uint32_t sh_bases;
+    uint32_t width, height, ss;
+    float focal_x, focal_y, center_x, center_y, far_plane;  // image pixels (resolve)
+    PassCamera cam;                                          // framebuffer (sample)
+    bool spatial_reuse;
+    int temporal_mode;
+};
+
+cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream);
+
+}  // namespace sgs
