@@ -72,7 +72,7 @@ typedef struct sgs_settings {
     const uint8_t* blue_noise;               /* (64, 128, 128) u8 volume, or NULL for white noise */
     const float* view_to_previous_view;      /* 4x4 row-major, read in REPROJECT mode; 16-byte aligned */
     uint32_t max_fragments;                  /* GPS points per Gaussian cap; 0 = W*H/2 as the reference */
-    uint32_t max_binned;                     /* hybrid GPS bin capacity; 0 = min(N, 2^20) as the reference */
+    uint32_t max_binned;                     /* hybrid bin capacity; 0 = min(N, 2^20) as the reference */
 } sgs_settings;
 
 /* Caller-owned state carried between calls (render.cu:38-43). */

@@ -79,6 +79,9 @@ int derive(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, D
                 d.queue_capacity = d.max_binned;
             }
         } else {
+            // the Gaussians the reference's hybrid pass gathers (accumulate_hybrid.cu:27,345)
+            if (s->hybrid_scheduling)
+                d.max_binned = std::min(s->max_binned != 0 ? s->max_binned : kDefaultMaxBinned, g->n_gaussians);
             d.queue_capacity = std::min(g->n_gaussians, kStQueueCapacity);
             const uint64_t limit = 0xffffffffull / std::max<uint64_t>(fbh, 1);
             if (d.queue_capacity > limit) d.queue_capacity = static_cast<uint32_t>(limit);
@@ -224,7 +227,7 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     w.q.count = reinterpret_cast<uint32_t*>(ws + F.q_count);
     w.q.capacity = d.queue_capacity;
 
-    cudaError_t err = launch_clear(w.framebuffer, d.n_fb, w.queue, stream);
+    cudaError_t err = launch_clear(w.framebuffer, d.n_fb, w.queue, sms, stream);
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "clear: %s", cudaGetErrorString(err));
 
     const PassCamera cam = pass_camera(c, s, d.ss);

@@ -16,7 +16,8 @@ struct WorkQueue {
     unsigned int next_chunk;     // work-stealing cursor of the consumer kernel
     unsigned int overflow;       // producers that found the queue full (processed in place)
     unsigned int error;          // nonzero when a consumer met an inconsistent entry
-    unsigned int pad[3];
+    unsigned int binned;         // hybrid ST: Gaussians the reference would gather, in arrival order
+    unsigned int pad[2];
 };
 constexpr unsigned long long kQueueEntryShift = 40;
 constexpr unsigned long long kQueueChunkMask = (1ull << kQueueEntryShift) - 1;
@@ -54,13 +55,14 @@ struct AccumulateParams {
     const uint8_t* blue_noise_slice;  // null: white noise
     uint32_t blue_noise_rotation;
     uint32_t max_fragments;           // GPS point cap per Gaussian
-    uint32_t max_binned;              // hybrid GPS: binned Gaussian capacity
+    uint32_t max_binned;              // hybrid: binned Gaussian capacity (accumulate_hybrid*.cu max_binned)
     bool hybrid;                      // hybrid scheduling
     WorkQueue* queue;
     QueueArrays q;
 };
 
-cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue* queue, cudaStream_t stream);
+cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue* queue, int num_sms,
+                         cudaStream_t stream);
 cudaError_t launch_accumulate_st(const AccumulateParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, int num_sms, cudaStream_t stream);
 
