@@ -106,6 +106,37 @@ struct RowSlot {
     uint4 c;   // opacity bits, key low, key high, blue-noise x offset | kGatherFormFlag
 };
 
+// Evaluates flattened position p (< total) of the row `r` that owns it (scatter_utils.cuh:35-46).
+// Positions past the end evaluate a valid pixel of the same row and do not merge.
+template <bool kBlue, bool kHybrid>
+__device__ __forceinline__ void st_position(const AccumulateParams& a, const RowSlot& r, const uint32_t p,
+                                            const uint32_t total) {
+    const float4 ra = r.a;
+    const uint4 rb = r.b;
+    const uint4 rc = r.c;
+    const bool in_range = p < total;
+    const uint32_t x = (in_range ? p : total - 1u) + rb.x;
+    const float dx = __fsub_rn(static_cast<float>(x), ra.x);
+    const float rdy = __uint_as_float(rb.w);
+    const float inner = __fmaf_rn(ra.y, dx, ra.z);
+    float e = __fmaf_rn(ra.w, rdy, __fmul_rn(dx, inner));
+    if (kHybrid && (rc.w & kGatherFormFlag)) e = __fmaf_rn(dx, inner, __fmul_rn(ra.w, rdy));
+    const float alpha = __fmul_rn(__uint_as_float(rc.x), exp2f(fminf(e, 0.0f)));
+    float u;
+    if (kBlue) {
+        const uint32_t texel = rb.z + ((x + (rc.w & 0x7fu)) % kBlueNoiseWidth);
+        const uint32_t value =
+            (static_cast<uint32_t>(a.blue_noise_slice[texel]) << 24u) + (1u << 23u) + a.blue_noise_rotation;
+        u = static_cast<float>(value >> 8u) * 5.9604644775390625e-8f;
+    } else {
+        u = __uint_as_float(0x3f800000u | (pcg_hash(rb.z ^ (x * 9277u)) >> 9u)) - 1.0f;
+    }
+    if (in_range && alpha >= kMinAlpha && u < alpha) {
+        const unsigned long long key = (static_cast<unsigned long long>(rc.z) << 32) | rc.y;
+        atomicMin(&a.framebuffer[rb.y + x], key);
+    }
+}
+
 // Each lane holds one row (valid) of Gaussian G at image row y. Computes the spans, lays the span
 // pixels of the 32 rows end to end and evaluates them with all lanes (scatter_utils.cuh:35-46).
 template <bool kBlue, bool kHybrid>
@@ -167,40 +198,20 @@ __device__ __forceinline__ void scatter_rows(const AccumulateParams& a, const ui
         s_rows[slot] = r;
     }
     __syncwarp();
+    // two positions per lane and step (p and p + 32): one pass over 64 positions; the body is
+    // straight-line code ending in one predicated RED
     int prev = -1;
-    for (uint32_t base = 0; base < total; base += 32) {
+    for (uint32_t base = 0; base < total; base += 64) {
         const uint32_t rel = first - base;
-        const uint32_t bits = __reduce_or_sync(kFullMask, (len > 0 && rel < 32u) ? (1u << rel) : 0u);
-        const int owner = prev + __popc(bits & upto_mask);
-        prev += __popc(bits);
-        const uint32_t p = base + lane;
-        if (p < total) {
-            const float4 ra = s_rows[owner].a;
-            const uint4 rb = s_rows[owner].b;
-            const uint4 rc = s_rows[owner].c;
-            const uint32_t x = p + rb.x;
-            const float dx = __fsub_rn(static_cast<float>(x), ra.x);
-            const float rdy = __uint_as_float(rb.w);
-            const float inner = __fmaf_rn(ra.y, dx, ra.z);
-            float e = __fmaf_rn(ra.w, rdy, __fmul_rn(dx, inner));
-            if (kHybrid && (rc.w & kGatherFormFlag)) e = __fmaf_rn(dx, inner, __fmul_rn(ra.w, rdy));
-            const float alpha = __fmul_rn(__uint_as_float(rc.x), exp2f(fminf(e, 0.0f)));
-            if (alpha >= kMinAlpha) {
-                float u;
-                if (kBlue) {
-                    const uint32_t texel = rb.z + ((x + (rc.w & 0x7fu)) % kBlueNoiseWidth);
-                    const uint32_t value = (static_cast<uint32_t>(a.blue_noise_slice[texel]) << 24u) + (1u << 23u) +
-                                           a.blue_noise_rotation;
-                    u = static_cast<float>(value >> 8u) * 5.9604644775390625e-8f;
-                } else {
-                    u = __uint_as_float(0x3f800000u | (pcg_hash(rb.z ^ (x * 9277u)) >> 9u)) - 1.0f;
-                }
-                if (u < alpha) {
-                    const unsigned long long key = (static_cast<unsigned long long>(rc.z) << 32) | rc.y;
-                    atomicMin(&a.framebuffer[rb.y + x], key);
-                }
-            }
-        }
+        const bool starts = len > 0 && rel < 64u;
+        const uint32_t bits_lo = __reduce_or_sync(kFullMask, (starts && rel < 32u) ? (1u << rel) : 0u);
+        const uint32_t bits_hi = __reduce_or_sync(kFullMask, (starts && rel >= 32u) ? (1u << (rel - 32u)) : 0u);
+        const int n_lo = __popc(bits_lo);
+        const int owner0 = prev + __popc(bits_lo & upto_mask);
+        const int owner1 = prev + n_lo + __popc(bits_hi & upto_mask);
+        prev += n_lo + __popc(bits_hi);
+        st_position<kBlue, kHybrid>(a, s_rows[owner0], base + lane, total);
+        st_position<kBlue, kHybrid>(a, s_rows[owner1], base + 32u + lane, total);
     }
     __syncwarp();
 }

@@ -291,6 +291,7 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     rp.far_plane = c->far_plane;
     rp.cam = cam;
     rp.spatial_reuse = s->spatial_reuse != 0;
+    rp.sh_vec4 = g->sh_bases == 16 && aligned16(g->sh_coefficients);
     rp.temporal_mode = s->temporal_mode;
     err = launch_sample_resolve(rp, stream);
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));

@@ -21,6 +21,49 @@ constexpr float kMinExtentLuma = 0.01f;
 constexpr float kMinExtentChroma = 0.005f;
 constexpr float kBorderMargin = 2.0f;
 
+// View-dependent colour of Gaussian g seen from the camera (resolve.cu:71-76).
+__device__ __forceinline__ float3 winner_color(const ResolveParams& a, const uint32_t g) {
+    const float vx = a.means[3 * g + 0] - a.cam_position[0];
+    const float vy = a.means[3 * g + 1] - a.cam_position[1];
+    const float vz = a.means[3 * g + 2] - a.cam_position[2];
+    const float inv_len = rsqrtf(vx * vx + vy * vy + vz * vz);
+    const float x = vx * inv_len, y = vy * inv_len, z = vz * inv_len;
+    if (a.sh_vec4) {
+        // 48 coefficients as twelve 16-byte loads
+        float c[48];
+        const float4* src = reinterpret_cast<const float4*>(a.sh + static_cast<size_t>(g) * 48);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+            const float4 v = __ldg(src + i);
+            c[4 * i + 0] = v.x;
+            c[4 * i + 1] = v.y;
+            c[4 * i + 2] = v.z;
+            c[4 * i + 3] = v.w;
+        }
+        return eval_sh(c, x, y, z, 16);
+    }
+    return eval_sh(a.sh + static_cast<size_t>(g) * a.sh_bases * 3, x, y, z, a.sh_bases);
+}
+
+// (rgb, depth) sample of a packed framebuffer entry, depth 0 = background (resolve.cu:65-78).
+// Neighbouring pixels mostly share their winner: one lane per distinct winner of the warp
+// evaluates the colour and shares it. Every lane of the warp must call this.
+__device__ __forceinline__ float4 warp_sample(const ResolveParams& a, const unsigned long long data,
+                                              const uint32_t lane) {
+    const uint32_t depth_key = static_cast<uint32_t>(data >> 32);
+    const bool has_sample = depth_key != 0xffffffffu;
+    const uint32_t g = static_cast<uint32_t>(data);
+    const uint32_t peers = __match_any_sync(0xffffffffu, has_sample ? g : 0xffffffffu);
+    const uint32_t leader = __ffs(peers) - 1;
+    float3 color = make_float3(0.0f, 0.0f, 0.0f);
+    if (has_sample && lane == leader) color = winner_color(a, g);
+    color.x = __shfl_sync(0xffffffffu, color.x, leader);
+    color.y = __shfl_sync(0xffffffffu, color.y, leader);
+    color.z = __shfl_sync(0xffffffffu, color.z, leader);
+    return has_sample ? make_float4(color.x, color.y, color.z, __uint_as_float(depth_key))
+                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 // Winner colour and depth per (sub)pixel; with spatial reuse also the resampling weights towards
 // the four neighbours and the k-buffer update (resolve.cu:27-144).
 template <bool kReuse>
@@ -33,16 +76,7 @@ __global__ void __launch_bounds__(kBlock) sample_kernel(const ResolveParams a) {
     const uint32_t depth_key = static_cast<uint32_t>(data >> 32);
     const bool has_sample = depth_key != 0xffffffffu;
     const uint32_t g = has_sample ? static_cast<uint32_t>(data) : 0u;
-    float4 sample = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (has_sample) {
-        const float vx = a.means[3 * g + 0] - a.cam_position[0];
-        const float vy = a.means[3 * g + 1] - a.cam_position[1];
-        const float vz = a.means[3 * g + 2] - a.cam_position[2];
-        const float inv_len = rsqrtf(vx * vx + vy * vy + vz * vz);
-        const float3 color = eval_sh(a.sh + static_cast<size_t>(g) * a.sh_bases * 3, vx * inv_len, vy * inv_len,
-                                     vz * inv_len, a.sh_bases);
-        sample = make_float4(color.x, color.y, color.z, __uint_as_float(depth_key));
-    }
+    const float4 sample = warp_sample(a, data, threadIdx.x & 31u);
     if (active) a.samples[pixel] = sample;
     if constexpr (!kReuse) return;
 
@@ -300,9 +334,76 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(const ResolveParams a) 
     a.weight_mass[pixel] = weight_mass;
 }
 
+// Sample and resolve in one pass when no neighbour is read (no spatial reuse, Reset or Static):
+// one thread per image pixel evaluates its ss x ss subpixels' winners (warp-deduplicated),
+// box-filters them and merges the history with resolve.cu:191-258's arithmetic. The samples are
+// still written for inspection.
+__global__ void __launch_bounds__(kBlock) sample_resolve_fused_kernel(const ResolveParams a) {
+    const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = idx < a.n_pixels;
+    const uint32_t pixel = active ? idx : a.n_pixels - 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ss = a.ss;
+    const uint32_t bx = (pixel % a.width) * ss;
+    const uint32_t by = (pixel / a.width) * ss;
+    const uint32_t fbw = a.width * ss;
+    const float norm = 1.0f / static_cast<float>(ss * ss);
+
+    float3 cs = make_float3(0.0f, 0.0f, 0.0f);
+    float ds = 0.0f, as = 0.0f, ws = 0.0f;
+    for (uint32_t oy = 0; oy < ss; ++oy) {
+        for (uint32_t ox = 0; ox < ss; ++ox) {
+            const uint32_t fi = (by + oy) * fbw + bx + ox;
+            const float4 s = warp_sample(a, a.framebuffer[fi], lane);
+            if (active) a.samples[fi] = s;
+            const float3 csum = make_float3(s.x, s.y, s.z);
+            const float dsum = s.w;
+            const float asum = s.w > 0.0f ? 1.0f : 0.0f;
+            const float wsum = 1.0f;
+            const float rcp = 1.0f / wsum;
+            cs.x += csum.x * rcp;
+            cs.y += csum.y * rcp;
+            cs.z += csum.z * rcp;
+            ds += dsum * rcp;
+            as += asum * rcp;
+            ws += wsum;
+        }
+    }
+    if (!active) return;
+    cs.x *= norm;
+    cs.y *= norm;
+    cs.z *= norm;
+    ds *= norm;
+    as *= norm;
+    ws *= norm;
+
+    float3 color = cs;
+    float depth = ds, alpha = as, weight_mass = ws;
+    if (a.temporal_mode == 1) {
+        const float hm = a.hist_weight_mass[pixel];
+        weight_mass = hm + ws;
+        const float hf = hm / weight_mass;
+        color.x = cs.x + hf * (a.hist_image[3 * pixel + 0] - cs.x);
+        color.y = cs.y + hf * (a.hist_image[3 * pixel + 1] - cs.y);
+        color.z = cs.z + hf * (a.hist_image[3 * pixel + 2] - cs.z);
+        depth = ds + hf * (a.hist_depth[pixel] - ds);
+        alpha = as + hf * (a.hist_alpha[pixel] - as);
+    }
+    a.image[3 * pixel + 0] = color.x;
+    a.image[3 * pixel + 1] = color.y;
+    a.image[3 * pixel + 2] = color.z;
+    a.depth[pixel] = depth;
+    a.alpha[pixel] = alpha;
+    a.weight_mass[pixel] = weight_mass;
+}
+
 }  // namespace
 
 cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream) {
+    if (!p.spatial_reuse && p.temporal_mode != 2) {
+        sample_resolve_fused_kernel<<<(p.n_pixels + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+        return cudaGetLastError();
+    }
     const unsigned grid_sample = (p.n_fb + kBlock - 1) / kBlock;
     const unsigned grid_resolve = (p.n_pixels + kBlock - 1) / kBlock;
     if (p.spatial_reuse) {

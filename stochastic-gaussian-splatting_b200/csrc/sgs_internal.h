@@ -95,6 +95,7 @@ struct ResolveParams {
     float focal_x, focal_y, center_x, center_y, far_plane;  // image pixels (resolve)
     PassCamera cam;                                          // framebuffer (sample)
     bool spatial_reuse;
+    bool sh_vec4;    // degree-3 SH at a 16-byte aligned base: winners load their coefficients as float4
     int temporal_mode;
 };
 
