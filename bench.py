@@ -1,0 +1,408 @@
+"""Benchmark of the per-sample stochastic render path: sample-frames/s at 1080p on 6M Gaussians.
+
+One step is one `_C.render` call (one stochastic sample merged progressively, Static resolve) of the
+synthetic 6M-Gaussian scene at 1920x1080: stochastic transparency, scatter scheduling, no
+supersampling. Inputs are resident in HBM; their 1.43 GB exceed the 126 MB L2, so no flush is done
+between steps. Prints one JSON line (see the keys below).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+--impl reference times the reference semantics on the host cores (the C++ restatement in oracle/,
+the reference having no CPU path) on the same workload. Multi-GPU runs are independent replicas, one
+per rank (the north-star path is single-GPU), timed on the device and reported as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "stochastic-gaussian-splatting_b200"))
+sys.path.insert(0, str(ROOT))
+
+import torch  # noqa: E402
+
+import sgs_scenes  # noqa: E402
+
+METRIC = "sample-frames/s at 1080p, 6M Gaussians"
+UNIT = "sample-frames/s"
+
+# name -> (scene, width, height, orbit radius, flags)
+WORKLOADS = {
+    "batch_6m_1080_st": ("batch_6m", 1920, 1080, 25.0, dict(aa=False, ss=1, gps=False, hybrid=False)),
+    "batch_6m_1080_gps": ("batch_6m", 1920, 1080, 25.0, dict(aa=False, ss=1, gps=True, hybrid=False)),
+    "batch_6m_4k_st": ("batch_6m", 3840, 2160, 25.0, dict(aa=False, ss=1, gps=False, hybrid=False)),
+    "st_100k_640_st": ("st_100k", 640, 480, 4.0, dict(aa=False, ss=1, gps=False, hybrid=False)),
+}
+DEFAULT_WORKLOAD = "batch_6m_1080_st"
+
+# DRAM bytes (read + write) of one st_scatter_kernel launch on the default workload, from
+# `ncu --set full` (profiles/st_scatter_kernel_batch_6m_1080.md)
+NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 278.47e6 + 16.60e6}
+
+# measured copy bandwidth of this pool's B200s when MEASURED_PEAKS.json is absent
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region (200 ms period)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    """The largest of the ranks' values (device time of the slowest replica)."""
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(steps_per_rank: int, world: int, max_elapsed_ms: float) -> float:
+    """Whole-job sample-frames/s of `world` independent replicas timed by the slowest one."""
+    return world * steps_per_rank / (max_elapsed_ms * 1e-3)
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def make_inputs(name: str):
+    scene_name, width, height, radius, flags = WORKLOADS[name]
+    scene = sgs_scenes.make_scene(sgs_scenes.SCENES[scene_name], seed=0)
+    cam = sgs_scenes.orbit_cameras(1, radius, width, height)[0] if radius != 4.0 else sgs_scenes.front_camera(width, height)
+    return scene, cam, flags
+
+
+def algorithmic_bytes(n: int, n_fb: int, n_px: int, unique_winners: int) -> dict:
+    """Bytes a sample-frame must move at least (plain path, Static resolve): Gaussian parameters read
+    once (44 B each), framebuffer clear + read (16 B per subpixel), samples written and read (32 B per
+    subpixel), history read and outputs written (48 B per pixel), winner means and SH gathered (204 B
+    per distinct winner)."""
+    accumulate = 44 * n + 8 * n_fb
+    frame = 44 * n + 48 * n_fb + 48 * n_px + 204 * unique_winners
+    return {"accumulate": accumulate, "frame": frame}
+
+
+def run_ours(args, world, rank, local) -> dict | None:
+    from StochasticGSCudaBackend import History, Settings, TemporalMode, _C, render
+
+    dev = torch.device("cuda", local)
+    scene_cpu, cam, fl = make_inputs(args.workload)
+    scene = scene_cpu.to(dev)
+    n = scene.means.shape[0]
+    W, H, ss = cam.width, cam.height, fl["ss"]
+    n_fb, n_px = W * H * ss * ss, W * H
+    w2c = cam.w2c.to(dev)
+    pos = cam.position.to(dev)
+    empty = torch.empty(0)
+    eye = torch.eye(4, device=dev)
+    blue = torch.empty(0, dtype=torch.uint8, device=dev)
+    kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device=dev), torch.empty((0, n_fb, 4), device=dev))
+    cam_args = (W, H, cam.focal_x, cam.focal_y, cam.center_x, cam.center_y, cam.near_plane, cam.far_plane)
+    flag_args = (fl["aa"], ss, fl["gps"], fl["hybrid"], False)
+
+    def step(hist, mode):
+        return _C.render(*scene.tensors(), w2c, pos, *cam_args, *flag_args, blue, *kb, *hist, eye, mode)
+
+    stream = torch.cuda.current_stream(dev)
+    hist = step((empty,) * 4, 0)
+    for _ in range(max(args.warmup, 3)):
+        hist = step(hist, 1)
+    torch.cuda.synchronize(dev)
+
+    # device-timed region: K steps, accumulate stage bracketed by events on the launching stream
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local))
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    t0.record(stream)
+    for k in range(args.steps):
+        _C.set_stage_events(starts[k], ends[k])
+        hist = step(hist, 1)
+    t1.record(stream)
+    _C.set_stage_events(None, None)
+    torch.cuda.synchronize(dev)
+    clock_info = clocks.stop()
+    barrier(world)
+    elapsed_ms = t0.elapsed_time(t1)
+    acc_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    acc_ms = max_over_ranks(acc_ms, world)
+
+    # one more sample for the algorithmic-byte count (distinct winners) and the launch count
+    _C.set_frame_index(_C.get_frame_index())
+    (_, _, _, _), ws, layout = _C.render_with_workspace(*scene.tensors(), w2c, pos, *cam_args, *flag_args, blue, *kb,
+                                                       *hist, eye, 1)
+    fb = _C.workspace_views(ws, layout, n_fb, False)["framebuffer"]
+    winners = fb[fb != -1]
+    unique = int(torch.unique(winners & 0xFFFFFFFF).numel())
+    alg = algorithmic_bytes(n, n_fb, n_px, unique)
+    launches_per_step = 2 + (2 if not fl["gps"] else (2 if fl["hybrid"] else 1))
+
+    # end to end through the public API: camera from pinned host memory, image back to pinned host memory
+    settings_host = (cam.w2c.pin_memory(), cam.position.pin_memory())
+    w2c_e = torch.empty_like(w2c)
+    pos_e = torch.empty_like(pos)
+    image_host = torch.empty((H, W, 3), dtype=torch.float32).pin_memory()
+    k_buffer = kb
+    hist_e = History(*hist)
+    for i in range(3):
+        w2c_e.copy_(settings_host[0], non_blocking=True)
+        pos_e.copy_(settings_host[1], non_blocking=True)
+        settings = Settings(w2c_e, pos_e, W, H, cam.focal_x, cam.focal_y, cam.center_x, cam.center_y,
+                            cam.near_plane, cam.far_plane, fl["aa"], ss, fl["gps"], fl["hybrid"], False)
+        hist_e = render(*scene.tensors(), settings, k_buffer, hist_e, eye, TemporalMode.STATIC)
+        image_host.copy_(hist_e.image, non_blocking=True)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        w2c_e.copy_(settings_host[0], non_blocking=True)
+        pos_e.copy_(settings_host[1], non_blocking=True)
+        settings = Settings(w2c_e, pos_e, W, H, cam.focal_x, cam.focal_y, cam.center_x, cam.center_y,
+                            cam.near_plane, cam.far_plane, fl["aa"], ss, fl["gps"], fl["hybrid"], False)
+        hist_e = render(*scene.tensors(), settings, k_buffer, hist_e, eye, TemporalMode.STATIC)
+        image_host.copy_(hist_e.image, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    h2d = w2c.numel() * 4 + pos.numel() * 4
+    d2h = H * W * 3 * 4
+
+    if rank != 0:
+        return None
+    peak, peak_kind = hbm_peak()
+    achieved = alg["accumulate"] / (acc_ms * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC_BYTES.get(args.workload)
+    ms_per_step = elapsed_ms / args.steps
+    value = replica_throughput(args.steps, world, elapsed_ms)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded 6M-Gaussian scene drawn as the batched-throughput workload; no dataset)",
+        "config": {
+            "workload": f"{args.workload}: {n} Gaussians, {W}x{H}, supersampling {ss}, "
+                        f"{'GPS' if fl['gps'] else 'stochastic transparency'}, "
+                        f"{'hybrid' if fl['hybrid'] else 'scatter'} scheduling, 1 spp per step, Static resolve",
+            "gaussians": n, "width": W, "height": H, "supersampling": ss, "use_gps": fl["gps"],
+            "hybrid_scheduling": fl["hybrid"], "spatial_reuse": False, "parallelism": f"replicas x{world}",
+            "l2": "inputs (1.43 GB) larger than L2 (126 MB), no flush",
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "accumulate stage (st_scatter_kernel + st_queue_kernel)" if not fl["gps"] else "accumulate stage (gps kernels)",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "peak_source": f"{peak_kind} hbm_gbs",
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg["accumulate"],
+            "accumulate_ms": round(acc_ms, 5),
+            "frame": {"algorithmic_bytes": alg["frame"], "achieved_gbs": round(alg["frame"] / (ms_per_step * 1e-3) / 1e9, 1),
+                      "frac": round(alg["frame"] / (ms_per_step * 1e-3) / 1e9 / peak, 4),
+                      "unique_winners": unique},
+        },
+        "e2e": {"value": round(replica_throughput(args.steps, world, e2e_ms), 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clock_info,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scene_cpu, cam, fl, args.cpu_frames, args.workload)
+    return line
+
+
+def cpu_baseline(scene_cpu, cam, fl, frames: int, workload: str) -> dict:
+    """The C++ restatement of the reference path (oracle/) on all host cores, a bounded sample."""
+    from oracle import cpu
+
+    threads = len(os.sched_getaffinity(0))
+    sc = {k: t.numpy() for k, t in zip(("means", "scales", "rotations", "opacities", "sh_coefficients"),
+                                       scene_cpu.tensors())}
+    cd = dict(width=cam.width, height=cam.height, focal_x=cam.focal_x, focal_y=cam.focal_y, center_x=cam.center_x,
+              center_y=cam.center_y, near_plane=cam.near_plane, far_plane=cam.far_plane, w2c=cam.w2c.numpy(),
+              position=cam.position.numpy())
+    hist = None
+    fb = cpu.accumulate(sc, cd, fl, 0, threads=threads)  # warm-up (page-in, thread pool)
+    t = time.perf_counter()
+    for f in range(frames):
+        fb = cpu.accumulate(sc, cd, fl, f + 1, threads=threads)
+        out = cpu.sample_resolve(sc, cd, fl, fb, history=hist, temporal_mode=1 if hist else 0, threads=threads)
+        hist = (out["image"], out["depth"], out["alpha"], out["weight_mass"])
+    dt = time.perf_counter() - t
+    return {"value": round(frames / dt, 4), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{frames} sample-frames of {workload} (accumulate + sample + resolve), {dt:.1f} s"}
+
+
+def run_reference(args, world, rank) -> dict | None:
+    if rank != 0:
+        return None
+    scene_cpu, cam, fl = make_inputs(args.workload)
+    from oracle import cpu
+
+    threads = len(os.sched_getaffinity(0))
+    sc = {k: t.numpy() for k, t in zip(("means", "scales", "rotations", "opacities", "sh_coefficients"),
+                                       scene_cpu.tensors())}
+    cd = dict(width=cam.width, height=cam.height, focal_x=cam.focal_x, focal_y=cam.focal_y, center_x=cam.center_x,
+              center_y=cam.center_y, near_plane=cam.near_plane, far_plane=cam.far_plane, w2c=cam.w2c.numpy(),
+              position=cam.position.numpy())
+    hist = None
+    frame = 0
+
+    def one():
+        nonlocal hist, frame
+        fb = cpu.accumulate(sc, cd, fl, frame, threads=threads)
+        out = cpu.sample_resolve(sc, cd, fl, fb, history=hist, temporal_mode=1 if hist else 0, threads=threads)
+        hist = (out["image"], out["depth"], out["alpha"], out["weight_mass"])
+        frame += 1
+
+    for _ in range(max(args.warmup, 1)):
+        one()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    dt = time.perf_counter() - t
+    value = args.steps / dt
+    return {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 6M-Gaussian scene)",
+        "config": {"workload": args.workload, "gaussians": int(scene_cpu.means.shape[0]), "width": cam.width,
+                   "height": cam.height, "parallelism": "host cores"},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full sample-frames of {args.workload}: the C++ restatement of the "
+                                   f"reference kernels (the reference has no CPU path)"},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--cpu-frames", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # reference semantics on the host cores; no GPU work, no process group needed
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        line = run_reference(args, world, rank)
+    else:
+        world, rank, local = dist_setup()
+        line = run_ours(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

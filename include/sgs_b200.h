@@ -119,6 +119,12 @@ int sgs_render(const sgs_gaussians* gaussians, const sgs_camera* camera, const s
                const sgs_history* history, const sgs_outputs* outputs, void* workspace, size_t workspace_bytes,
                void* stream);
 
+/* Diagnostics (no counterpart in the reference): CUDA events (cudaEvent_t) that the calling
+ * thread's next sgs_render calls record on their stream immediately before the first and after the
+ * last kernel of the accumulate stage, so that callers can time that stage with cudaEventElapsedTime.
+ * NULL, NULL disables the recording. */
+void sgs_set_stage_events(void* accumulate_start, void* accumulate_end);
+
 /* Process-wide frame index (render.cu:56-57 keeps it in a hidden static counter that starts at 0);
  * exposed so that random streams can be pinned and resumed. */
 uint32_t sgs_get_frame_index(void);

@@ -35,6 +35,12 @@ def set_frame_index(frame_index: int) -> None:
     _lib.sgs_set_frame_index(int(frame_index) & 0xFFFFFFFF)
 
 
+def set_stage_events(start=None, end=None) -> None:
+    """Records `start`/`end` (torch.cuda.Event) around the accumulate stage of this thread's next
+    render calls; None disables. Timing aid (no counterpart in the reference module)."""
+    _lib.sgs_set_stage_events(None if start is None else start.cuda_event, None if end is None else end.cuda_event)
+
+
 def _check(cond: bool, msg: str) -> None:
     if not cond:
         raise RuntimeError(msg)

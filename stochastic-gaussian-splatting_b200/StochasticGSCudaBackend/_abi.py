@@ -97,6 +97,7 @@ SIGNATURES = {
     "sgs_render": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC),
                                   ctypes.POINTER(HistoryC), ctypes.POINTER(Outputs), ctypes.c_void_p, ctypes.c_size_t,
                                   ctypes.c_void_p]),
+    "sgs_set_stage_events": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_get_frame_index": (ctypes.c_uint32, []),
     "sgs_set_frame_index": (None, [ctypes.c_uint32]),
     "sgs_k_buffer_size": (ctypes.c_uint32, []),
@@ -119,7 +120,7 @@ def load() -> ctypes.CDLL:
         return _lib
     path = library_path()
     if not path.is_file():
-        raise ImportError(f"{path} is missing: build it with `python stochastic-gaussian-splatting_b200/build.py`")
+        raise ImportError(f"{path} is missing: build it with `python stochastic-gaussian-splatting_b200/sgs_build.py`")
     lib = ctypes.CDLL(str(path))
     for name, (restype, argtypes) in SIGNATURES.items():
         fn = getattr(lib, name)

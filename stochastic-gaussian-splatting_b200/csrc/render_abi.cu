@@ -21,6 +21,9 @@ using namespace sgs;
 
 std::atomic<uint32_t> g_frame_index{0};
 thread_local std::string t_last_error;
+// optional accumulate-stage events (sgs_set_stage_events)
+thread_local cudaEvent_t t_stage_start = nullptr;
+thread_local cudaEvent_t t_stage_end = nullptr;
 
 constexpr size_t kAlign = 256;
 constexpr uint32_t kDefaultMaxBinned = 1u << 20;     // accumulate_hybrid_gps.cu:22
@@ -252,7 +255,9 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
         ap.hybrid = s->hybrid_scheduling != 0;
         ap.queue = w.queue;
         ap.q = w.q;
+        if (t_stage_start != nullptr) cudaEventRecord(t_stage_start, stream);
         err = s->use_gps ? launch_accumulate_gps(ap, sms, stream) : launch_accumulate_st(ap, sms, stream);
+        if (t_stage_end != nullptr && err == cudaSuccess) err = cudaEventRecord(t_stage_end, stream);
         if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "accumulate: %s", cudaGetErrorString(err));
     }
 
@@ -296,6 +301,11 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     err = launch_sample_resolve(rp, stream);
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));
     return SGS_OK;
+}
+
+void sgs_set_stage_events(void* accumulate_start, void* accumulate_end) {
+    t_stage_start = static_cast<cudaEvent_t>(accumulate_start);
+    t_stage_end = static_cast<cudaEvent_t>(accumulate_end);
 }
 
 uint32_t sgs_get_frame_index(void) { return g_frame_index.load(std::memory_order_relaxed); }

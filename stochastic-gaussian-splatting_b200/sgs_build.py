@@ -5,7 +5,7 @@ the bit-exact parity of the winners relies on) plus -lineinfo for profiling, the
 C-ABI shared library (include/sgs_b200.h) with the CUDA runtime linked statically. Objects go to
 _build/; the library is written in-tree so that it ships with the package.
 
-    python stochastic-gaussian-splatting_b200/build.py [-v] [--ptxas-info]
+    python stochastic-gaussian-splatting_b200/sgs_build.py [-v] [--ptxas-info]
 """
 from __future__ import annotations
 

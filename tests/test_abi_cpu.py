@@ -1,0 +1,143 @@
+"""The C ABI library on a machine without a GPU: symbols, struct layout, validation, frame index."""
+import ctypes
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from StochasticGSCudaBackend import _abi
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "sgs_b200.h"
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:[a-z_0-9 ]+\*?\s*)\b(sgs_[a-z_0-9]+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_function():
+    lib = _abi.load()
+    names = declared_functions()
+    assert len(names) >= 9, names
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(_abi.SIGNATURES), "ctypes declarations out of sync with the header"
+
+
+def test_struct_layout_matches_the_header(tmp_path):
+    """ctypes structures have the sizes and offsets a C compiler gives the header's structs."""
+    structs = {
+        "sgs_gaussians": _abi.Gaussians, "sgs_camera": _abi.Camera, "sgs_settings": _abi.SettingsC,
+        "sgs_history": _abi.HistoryC, "sgs_outputs": _abi.Outputs, "sgs_workspace_layout": _abi.WorkspaceLayout,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void) {']
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'printf("{cname}.{field} %zu\\n", offsetof({cname}, {field}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    cc = shutil.which("gcc") or "gcc"
+    exe = tmp_path / "layout"
+    subprocess.run([cc, str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                               check=True).stdout.splitlines())
+    for cname, cls in structs.items():
+        assert int(out[cname]) == ctypes.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert int(out[f"{cname}.{field}"]) == getattr(cls, field).offset, f"{cname}.{field}"
+
+
+def _args(n=10, width=64, height=48, ss=1, mode=0, reuse=0, gps=0, hybrid=0):
+    fake = 0x10000  # never dereferenced: validation fails or sizes are computed before any launch
+    g = _abi.Gaussians(fake, fake, fake, fake, fake, n, 16)
+    c = _abi.Camera(fake, fake, width, height, 50.0, 50.0, width / 2, height / 2, 0.2, 100.0)
+    s = _abi.SettingsC(0, ss, gps, hybrid, reuse, mode, None, None, 0, 0)
+    return g, c, s
+
+
+def test_workspace_size_and_layout():
+    lib = _abi.load()
+    g, c, s = _args(n=1000, width=640, height=480)
+    size = lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s))
+    lay = _abi.WorkspaceLayout()
+    assert lib.sgs_get_workspace_layout(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(lay)) == 0
+    assert lay.total == size
+    n_fb = 640 * 480
+    assert lay.samples - lay.framebuffer >= 8 * n_fb
+    assert all(v % 256 == 0 for v in (lay.framebuffer, lay.samples, lay.reuse_weights, lay.queue, lay.total))
+    g2, c2, s2 = _args(n=1000, width=640, height=480, ss=2, reuse=1)
+    size2 = lib.sgs_workspace_size(ctypes.byref(g2), ctypes.byref(c2), ctypes.byref(s2))
+    assert size2 >= 4 * 40 * n_fb  # fb + samples + reuse weights at 4x the subpixels
+
+
+def test_invalid_arguments_are_rejected_before_any_launch():
+    lib = _abi.load()
+    h = _abi.HistoryC()
+    o = _abi.Outputs(0x10000, 0x10000, 0x10000, 0x10000)
+
+    def call(g, c, s, ws=0x100000, nbytes=1 << 40):
+        st = lib.sgs_render(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h), ctypes.byref(o),
+                            ctypes.c_void_p(ws), ctypes.c_size_t(nbytes), None)
+        return st, _abi.last_error(lib)
+
+    g, c, s = _args(mode=7)
+    st, msg = call(g, c, s)
+    assert st == _abi.SGS_ERROR_INVALID_ARGUMENT and "temporal mode" in msg
+    g, c, s = _args(width=0)
+    assert call(g, c, s)[0] == _abi.SGS_ERROR_INVALID_ARGUMENT
+    g, c, s = _args()
+    g.sh_bases = 5
+    assert "sh_bases" in call(g, c, s)[1]
+    g, c, s = _args(mode=1)  # STATIC without a history
+    assert call(g, c, s)[0] == _abi.SGS_ERROR_INVALID_ARGUMENT
+    g, c, s = _args(reuse=1)  # spatial reuse without k-buffers
+    assert call(g, c, s)[0] == _abi.SGS_ERROR_INVALID_ARGUMENT
+    g, c, s = _args()
+    g.rotations = 0x10004  # misaligned quaternions
+    assert "aligned" in call(g, c, s)[1]
+    g, c, s = _args()
+    assert call(g, c, s, ws=0x100010)[0] == _abi.SGS_ERROR_WORKSPACE  # misaligned workspace
+    assert call(g, c, s, nbytes=16)[0] == _abi.SGS_ERROR_WORKSPACE  # too small
+    g, c, s = _args(width=1 << 23, height=1 << 12, ss=4)  # framebuffer side beyond exact float range
+    assert call(g, c, s)[0] == _abi.SGS_ERROR_INVALID_ARGUMENT
+
+
+def test_frame_index_and_constants():
+    lib = _abi.load()
+    assert lib.sgs_k_buffer_size() == 4
+    assert lib.sgs_abi_version() == _abi.ABI_VERSION
+    lib.sgs_set_frame_index(123)
+    assert lib.sgs_get_frame_index() == 123
+    lib.sgs_set_frame_index(0xFFFFFFFF)
+    assert lib.sgs_get_frame_index() == 0xFFFFFFFF
+    lib.sgs_set_frame_index(0)
+
+
+def test_python_module_mirrors_the_reference_binding():
+    import inspect
+
+    import torch
+
+    from StochasticGSCudaBackend import History, Settings, TemporalMode, _C, create_k_buffer, render
+
+    assert _C.k_buffer_size == 4
+    assert Settings._fields == ("w2c", "cam_position", "width", "height", "focal_x", "focal_y", "center_x",
+                                "center_y", "near_plane", "far_plane", "proper_antialiasing", "supersampling_factor",
+                                "use_gps", "hybrid_scheduling", "spatial_reuse")
+    assert [m.name for m in TemporalMode] == ["RESET", "STATIC", "REPROJECT"] and int(TemporalMode.REPROJECT) == 2
+    assert History._fields == ("image", "depth", "alpha", "weight_mass")
+    assert list(inspect.signature(render).parameters) == ["means", "scales", "rotations", "opacities",
+                                                          "sh_coefficients", "settings", "k_buffer", "history",
+                                                          "view_to_previous_view", "temporal_mode"]
+    assert callable(create_k_buffer)
+    with pytest.raises(TypeError):
+        _C.render(1, 2, 3)
+    cpu = torch.zeros(4, 3)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        _C.render(cpu, cpu, cpu, cpu, cpu, cpu, cpu, 4, 4, 1.0, 1.0, 2.0, 2.0, 0.1, 10.0, False, 1, False, False,
+                  False, torch.empty(0), cpu, cpu, cpu, cpu, cpu, cpu, cpu, 0)
