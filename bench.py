@@ -46,7 +46,7 @@ DEFAULT_WORKLOAD = "batch_6m_1080_st"
 
 # DRAM bytes (read + write) of one st_scatter_kernel launch on the default workload, from
 # `ncu --set full` (profiles/st_scatter_kernel_batch_6m_1080.md)
-NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 278.47e6 + 16.60e6}
+NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 278.58e6 + 15.51e6}
 
 # measured copy bandwidth of this pool's B200s when MEASURED_PEAKS.json is absent
 FALLBACK_HBM_GBS = 6650.0
@@ -109,6 +109,35 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+class RawEvents:
+    """cudaEvent_t handles from the CUDA runtime already loaded by torch, for events that the render
+    library records itself (torch only times events it recorded)."""
+
+    def __init__(self):
+        import ctypes
+
+        self.ct = ctypes
+        self.rt = ctypes.CDLL("libcudart.so.12")
+        self.rt.cudaEventCreate.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+        self.rt.cudaEventElapsedTime.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.c_void_p]
+        self.rt.cudaEventDestroy.argtypes = [ctypes.c_void_p]
+
+    def create(self):
+        ev = self.ct.c_void_p()
+        if self.rt.cudaEventCreate(self.ct.byref(ev)) != 0:
+            raise RuntimeError("cudaEventCreate failed")
+        return ev
+
+    def elapsed_ms(self, start, end) -> float:
+        ms = self.ct.c_float()
+        if self.rt.cudaEventElapsedTime(self.ct.byref(ms), start, end) != 0:
+            raise RuntimeError("cudaEventElapsedTime failed")
+        return ms.value
+
+    def destroy(self, ev):
+        self.rt.cudaEventDestroy(ev)
 
 
 def dist_setup():
@@ -194,8 +223,9 @@ def run_ours(args, world, rank, local) -> dict | None:
     torch.cuda.synchronize(dev)
 
     # device-timed region: K steps, accumulate stage bracketed by events on the launching stream
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    raw = RawEvents()
+    starts = [raw.create() for _ in range(args.steps)]
+    ends = [raw.create() for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     props = torch.cuda.get_device_properties(dev)
     clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local))
@@ -213,7 +243,9 @@ def run_ours(args, world, rank, local) -> dict | None:
     clock_info = clocks.stop()
     barrier(world)
     elapsed_ms = t0.elapsed_time(t1)
-    acc_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+    acc_ms = sum(raw.elapsed_ms(s, e) for s, e in zip(starts, ends)) / args.steps
+    for ev in starts + ends:
+        raw.destroy(ev)
     elapsed_ms = max_over_ranks(elapsed_ms, world)
     acc_ms = max_over_ranks(acc_ms, world)
 

@@ -36,9 +36,9 @@ def set_frame_index(frame_index: int) -> None:
 
 
 def set_stage_events(start=None, end=None) -> None:
-    """Records `start`/`end` (torch.cuda.Event) around the accumulate stage of this thread's next
-    render calls; None disables. Timing aid (no counterpart in the reference module)."""
-    _lib.sgs_set_stage_events(None if start is None else start.cuda_event, None if end is None else end.cuda_event)
+    """Records `start`/`end` (cudaEvent_t handles as int or c_void_p) around the accumulate stage of
+    this thread's next render calls; None disables. Timing aid (no counterpart in the reference module)."""
+    _lib.sgs_set_stage_events(start, end)
 
 
 def _check(cond: bool, msg: str) -> None:
