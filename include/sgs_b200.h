@@ -119,6 +119,20 @@ int sgs_render(const sgs_gaussians* gaussians, const sgs_camera* camera, const s
                const sgs_history* history, const sgs_outputs* outputs, void* workspace, size_t workspace_bytes,
                void* stream);
 
+/* sgs_render for callers that cannot allocate device memory while rendering (a plugin inside a
+ * host application under a fixed memory budget, a C caller without a caching allocator). It has no
+ * counterpart in the reference. The caller passes inputs, history and outputs as for sgs_render;
+ * the scratch lives in a fixed 64 MiB device array of the library instead of a caller workspace,
+ * so nothing is allocated per call. That array is held by every CUDA context that loads it, until
+ * the process exits. The first call on each device (that device current) looks up the array's
+ * device address; make it before any stream capture. All calls on a device share the array: the
+ * render clears what must start empty, but calls that can overlap on the GPU race and must be
+ * ordered by the caller. Renders needing more than 64 MiB of scratch (sgs_workspace_size) are
+ * rejected with SGS_ERROR_WORKSPACE before any launch; 1920x1080 without supersampling or spatial
+ * reuse fits. */
+int sgs_render_no_alloc(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                        const sgs_history* history, const sgs_outputs* outputs, void* stream);
+
 /* Diagnostics (no counterpart in the reference): CUDA events (cudaEvent_t) that the calling
  * thread's next sgs_render calls record on their stream immediately before the first and after the
  * last kernel of the accumulate stage, so that callers can time that stage with cudaEventElapsedTime.

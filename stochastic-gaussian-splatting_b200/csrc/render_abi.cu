@@ -161,6 +161,16 @@ PassCamera pass_camera(const sgs_camera* c, const sgs_settings* s, const uint32_
 
 }  // namespace
 
+int sgs::record_error(const int status, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return status;
+}
+
 extern "C" {
 
 size_t sgs_workspace_size(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings) {

@@ -101,4 +101,7 @@ struct ResolveParams {
 
 cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream);
 
+// Sets the calling thread's sgs_last_error() message (printf format) and returns `status`.
+int record_error(int status, const char* fmt, ...);
+
 }  // namespace sgs
