@@ -340,9 +340,49 @@ def run_ours(args, world, rank, local) -> dict | None:
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clock_info,
     }
+    if not args.no_batch and args.workload.startswith("batch_6m"):
+        line["batch32_graph"] = batch_graph(scene, fl, dev, steps=max(4, args.steps // 8))
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_cpu, cam, fl, args.cpu_frames, args.workload)
     return line
+
+
+def batch_graph(scene, fl, dev, steps: int) -> dict:
+    """32 views cycling 720p, 1080p, 1440p and 4K on the orbit, one sample each, captured in one CUDA
+    graph (the batched-throughput workload); also the same 32 calls made eagerly."""
+    import sgs_batch
+
+    res = [(1280, 720), (1920, 1080), (2560, 1440), (3840, 2160)]
+    views = sgs_batch.batch_views(32, 25.0, res)
+    batch = sgs_batch.CapturedViews(scene.tensors(), views, fl, first_frame=1 << 20, device=dev).capture()
+    for _ in range(2):
+        batch.replay()
+    stream = torch.cuda.current_stream(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    t0.record(stream)
+    for _ in range(steps):
+        batch.replay()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    graph_ms = t0.elapsed_time(t1) / steps
+    hist = [tuple(h) for h in batch.static_out]
+    for _ in range(2):
+        hist = batch._render_all(hist, 1)
+    torch.cuda.synchronize(dev)
+    t0.record(stream)
+    for _ in range(steps):
+        hist = batch._render_all(hist, 1)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    eager_ms = t0.elapsed_time(t1) / steps
+    pixels = sum(w * h for w, h in res) * 8
+    del batch
+    torch.cuda.empty_cache()
+    return {"views": 32, "resolutions": "1280x720, 1920x1080, 2560x1440, 3840x2160 (8 each)",
+            "ms_per_batch_graph": round(graph_ms, 4), "ms_per_batch_eager": round(eager_ms, 4),
+            "sample_frames_per_s_graph": round(32 / (graph_ms * 1e-3), 1),
+            "megapixels_per_s_graph": round(pixels / (graph_ms * 1e-3) / 1e6, 1)}
 
 
 def cpu_baseline(scene_cpu, cam, fl, frames: int, workload: str) -> dict:
@@ -419,6 +459,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 32-view CUDA-graph measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         # reference semantics on the host cores; no GPU work, no process group needed

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define SGS_ABI_VERSION 1
+#define SGS_ABI_VERSION 2
 #define SGS_K_BUFFER_SIZE 4 /* k-buffer entries per (sub)pixel, resolve.h:9 / render.cu:164 */
 
 enum sgs_status {
@@ -73,6 +73,10 @@ typedef struct sgs_settings {
     const float* view_to_previous_view;      /* 4x4 row-major, read in REPROJECT mode; 16-byte aligned */
     uint32_t max_fragments;                  /* GPS points per Gaussian cap; 0 = W*H/2 as the reference */
     uint32_t max_binned;                     /* hybrid bin capacity; 0 = min(N, 2^20) as the reference */
+    uint32_t* frame_index_device;            /* NULL: the process-wide frame index (render.cu:56-57); else a
+                                                device word the call reads as its frame index and advances
+                                                by one on the GPU, so that calls captured in a CUDA graph
+                                                draw new random numbers on every replay */
 } sgs_settings;
 
 /* Caller-owned state carried between calls (render.cu:38-43). */

@@ -35,6 +35,37 @@ def set_frame_index(frame_index: int) -> None:
     _lib.sgs_set_frame_index(int(frame_index) & 0xFFFFFFFF)
 
 
+_device_frame_counters: dict = {}
+
+
+def set_device_frame_counter(counter: torch.Tensor | None, device=None) -> None:
+    """Keeps the frame index of subsequent calls on `counter`'s device in that one-element int32 CUDA
+    tensor: each call reads it as its frame index and advances it on the GPU, so render calls
+    captured in a CUDA graph draw new random numbers on every replay. None returns that device to
+    the process-wide counter (`get_frame_index`). The tensor must stay alive while it is in use."""
+    if counter is None:
+        _device_frame_counters.pop(_device_key(device), None)
+        return
+    _check(counter.is_cuda and counter.dtype == torch.int32 and counter.numel() == 1 and counter.is_contiguous(),
+           "the frame counter must be a contiguous one-element int32 CUDA tensor")
+    _device_frame_counters[_device_key(counter.device)] = counter
+
+
+def _device_key(device) -> int:
+    """CUDA device ordinal of `device` (None, "cuda", "cuda:1", torch.device or int)."""
+    if device is None:
+        return torch.cuda.current_device()
+    if isinstance(device, int):
+        return device
+    d = torch.device(device)
+    return d.index if d.index is not None else torch.cuda.current_device()
+
+
+def _device_frame_pointer(device: torch.device) -> int | None:
+    t = _device_frame_counters.get(_device_key(device))
+    return None if t is None else t.data_ptr()
+
+
 def set_stage_events(start=None, end=None) -> None:
     """Records `start`/`end` (cudaEvent_t handles as int or c_void_p) around the accumulate stage of
     this thread's next render calls; None disables. Timing aid (no counterpart in the reference module)."""
@@ -121,7 +152,8 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
     c = _abi.Camera(w2c.data_ptr(), cam_position.data_ptr(), width, height, float(focal_x), float(focal_y),
                     float(center_x), float(center_y), float(near_plane), float(far_plane))
     s = _abi.SettingsC(int(bool(proper_antialiasing)), ss, int(bool(use_gps)), int(bool(hybrid_scheduling)),
-                       int(bool(spatial_reuse)), mode, _ptr(blue_noise), _ptr(view_to_previous_view), 0, 0)
+                       int(bool(spatial_reuse)), mode, _ptr(blue_noise), _ptr(view_to_previous_view), 0, 0,
+                       _device_frame_pointer(device))
     h = _abi.HistoryC(
         _ptr(history_image) if mode else None, _ptr(history_depth) if mode else None,
         _ptr(history_alpha) if mode else None, _ptr(history_weight_mass) if mode else None,

@@ -9,7 +9,7 @@ import ctypes
 from pathlib import Path
 
 LIB_NAME = "libsgs_b200.so"
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 SGS_OK = 0
 SGS_ERROR_INVALID_ARGUMENT = -1
@@ -56,6 +56,7 @@ class SettingsC(ctypes.Structure):
         ("view_to_previous_view", ctypes.c_void_p),
         ("max_fragments", ctypes.c_uint32),
         ("max_binned", ctypes.c_uint32),
+        ("frame_index_device", ctypes.c_void_p),
     ]
 
 

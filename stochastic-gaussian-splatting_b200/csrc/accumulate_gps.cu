@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     PointSource s;
     s.opacity_dilog = gps_dilog(p.opacity);
     const float importance = kTwoPi * sqrtf(p.determinant) * s.opacity_dilog;
-    uint2 seed = gps_seed(g, a.frame_idx);
+    uint2 seed = gps_seed(g, frame_rng(a).frame);
     const uint32_t true_count = poisson_count(seed, importance);
     if (true_count == 0) active = false;
     const uint32_t cap = a.max_fragments != 0
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParam
         s.conic = make_float3(__uint_as_float(m.x), __uint_as_float(m.y), __uint_as_float(m.z));
         const uint32_t n_points = a.q.count[lo];
         const uint32_t gaussian = static_cast<uint32_t>(s.key);
-        const uint2 base_seed = gps_seed(gaussian, a.frame_idx);
+        const uint2 base_seed = gps_seed(gaussian, frame_rng(a).frame);
         const uint32_t first_point = (c - m.w) * kChunkPoints;
         for (uint32_t k = lane; k < kChunkPoints; k += 32) {
             const uint32_t point = first_point + k;

@@ -109,8 +109,8 @@ struct RowSlot {
 // Evaluates flattened position p (< total) of the row `r` that owns it (scatter_utils.cuh:35-46).
 // Positions past the end evaluate a valid pixel of the same row and do not merge.
 template <bool kBlue, bool kHybrid>
-__device__ __forceinline__ void st_position(const AccumulateParams& a, const RowSlot& r, const uint32_t p,
-                                            const uint32_t total) {
+__device__ __forceinline__ void st_position(const AccumulateParams& a, const FrameRng& rng, const RowSlot& r,
+                                            const uint32_t p, const uint32_t total) {
     const float4 ra = r.a;
     const uint4 rb = r.b;
     const uint4 rc = r.c;
@@ -126,7 +126,7 @@ __device__ __forceinline__ void st_position(const AccumulateParams& a, const Row
     if (kBlue) {
         const uint32_t texel = rb.z + ((x + (rc.w & 0x7fu)) % kBlueNoiseWidth);
         const uint32_t value =
-            (static_cast<uint32_t>(a.blue_noise_slice[texel]) << 24u) + (1u << 23u) + a.blue_noise_rotation;
+            (static_cast<uint32_t>(rng.slice[texel]) << 24u) + (1u << 23u) + rng.rotation;
         u = static_cast<float>(value >> 8u) * 5.9604644775390625e-8f;
     } else {
         u = __uint_as_float(0x3f800000u | (pcg_hash(rb.z ^ (x * 9277u)) >> 9u)) - 1.0f;
@@ -140,9 +140,9 @@ __device__ __forceinline__ void st_position(const AccumulateParams& a, const Row
 // Each lane holds one row (valid) of Gaussian G at image row y. Computes the spans, lays the span
 // pixels of the 32 rows end to end and evaluates them with all lanes (scatter_utils.cuh:35-46).
 template <bool kBlue, bool kHybrid>
-__device__ __forceinline__ void scatter_rows(const AccumulateParams& a, const uint32_t lane, const uint32_t lt_mask,
-                                             const uint32_t upto_mask, RowSlot* s_rows, const bool valid,
-                                             const RowGaussian& G, const uint32_t y) {
+__device__ __forceinline__ void scatter_rows(const AccumulateParams& a, const FrameRng& rng, const uint32_t lane,
+                                             const uint32_t lt_mask, const uint32_t upto_mask, RowSlot* s_rows,
+                                             const bool valid, const RowGaussian& G, const uint32_t y) {
     uint32_t xs = 0, len = 0;
     float dy = 0.0f, cydy = 0.0f, czdy = 0.0f;
     if (valid) {
@@ -189,7 +189,7 @@ __device__ __forceinline__ void scatter_rows(const AccumulateParams& a, const ui
             bx = (G.key_lo * 0xC13FA9A9u) >> 25u;
             seed = ((y + oy) % kBlueNoiseHeight) * kBlueNoiseWidth;
         } else {
-            seed = G.key_lo ^ (a.frame_idx * 1973u) ^ (y * 2699u);
+            seed = G.key_lo ^ (rng.frame * 1973u) ^ (y * 2699u);
         }
         RowSlot r;
         r.a = make_float4(G.mx, G.cx, cydy, czdy);
@@ -210,8 +210,8 @@ __device__ __forceinline__ void scatter_rows(const AccumulateParams& a, const ui
         const int owner0 = prev + __popc(bits_lo & upto_mask);
         const int owner1 = prev + n_lo + __popc(bits_hi & upto_mask);
         prev += n_lo + __popc(bits_hi);
-        st_position<kBlue, kHybrid>(a, s_rows[owner0], base + lane, total);
-        st_position<kBlue, kHybrid>(a, s_rows[owner1], base + 32u + lane, total);
+        st_position<kBlue, kHybrid>(a, rng, s_rows[owner0], base + lane, total);
+        st_position<kBlue, kHybrid>(a, rng, s_rows[owner1], base + 32u + lane, total);
     }
     __syncwarp();
 }
@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
 
     Projected p;
     if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p)) return;
+    const FrameRng rng = frame_rng(a);
 
     const PixelRect rect = pixel_rect(p.bounds, a.cam);
     const uint32_t count = active ? rect.width * rect.height : 0u;
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         const bool valid = r < total_rows;
         const RowGaussian rg = s_gauss[wib][valid ? owner : 0];
         const uint32_t y = rg.y_min + (r - rg.row_first);
-        scatter_rows<kBlue, kHybrid>(a, lane, lt_mask, upto_mask, s_rows[wib], valid, rg, y);
+        scatter_rows<kBlue, kHybrid>(a, rng, lane, lt_mask, upto_mask, s_rows[wib], valid, rg, y);
     }
 
     // queue overflow: the warp processes its kept large Gaussians, 32 rows at a time
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         const RowGaussian bg = s_gauss[wib][0];
         for (uint32_t r0 = 0; r0 < bh; r0 += 32) {
             const bool valid = r0 + lane < bh;
-            scatter_rows<kBlue, kHybrid>(a, lane, lt_mask, upto_mask, s_rows[wib], valid, bg, bg.y_min + r0 + lane);
+            scatter_rows<kBlue, kHybrid>(a, rng, lane, lt_mask, upto_mask, s_rows[wib], valid, bg, bg.y_min + r0 + lane);
         }
     }
 }
@@ -340,6 +341,7 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t upto_mask = kFullMask >> (31u - lane);
     const unsigned long long packed = a.queue->packed;
+    const FrameRng rng = frame_rng(a);
     const uint32_t n_entries =
         static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(a.q.capacity)));
     if (n_entries == 0) return;
@@ -386,7 +388,7 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
         const uint32_t r1 = min(r0 + rpc, m.y);
         for (uint32_t r = r0; r < r1; r += 32) {
             const bool valid = r + lane < r1;
-            scatter_rows<kBlue, kHybrid>(a, lane, lt_mask, upto_mask, s_rows[wib], valid, G, G.y_min + r + lane);
+            scatter_rows<kBlue, kHybrid>(a, rng, lane, lt_mask, upto_mask, s_rows[wib], valid, G, G.y_min + r + lane);
         }
     }
 }
@@ -431,7 +433,7 @@ cudaError_t launch_accumulate_st(const AccumulateParams& p, const int num_sms, c
     if (p.n == 0) return cudaSuccess;
     const unsigned grid = (p.n + kBlock - 1) / kBlock;
     const unsigned queue_grid = static_cast<unsigned>(num_sms) * kQueueBlocksPerSM;
-    const bool blue = p.blue_noise_slice != nullptr;
+    const bool blue = p.blue_noise != nullptr;
     if (blue && p.hybrid) launch_st<true, true>(p, grid, queue_grid, stream);
     else if (blue) launch_st<true, false>(p, grid, queue_grid, stream);
     else if (p.hybrid) launch_st<false, true>(p, grid, queue_grid, stream);

@@ -225,7 +225,9 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
 
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     char* ws = static_cast<char*>(workspace);
-    const uint32_t frame = g_frame_index.fetch_add(1u, std::memory_order_relaxed);
+    // the host counter serves calls that keep no frame index in device memory
+    const uint32_t frame =
+        s->frame_index_device != nullptr ? 0u : g_frame_index.fetch_add(1u, std::memory_order_relaxed);
     const int sms = sm_count();
 
     Workspace w{};
@@ -254,12 +256,10 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
         ap.framebuffer = w.framebuffer;
         ap.n = g->n_gaussians;
         ap.frame_idx = frame;
+        ap.frame_ptr = s->frame_index_device;
         ap.cam = cam;
-        // one blue-noise slice per frame, each pass through the volume rotated by the golden ratio
-        ap.blue_noise_slice = s->blue_noise != nullptr && !s->use_gps
-                                  ? s->blue_noise + static_cast<size_t>(frame % kBlueNoiseDepth) * kBlueNoiseWidth * kBlueNoiseHeight
-                                  : nullptr;
-        ap.blue_noise_rotation = (frame / kBlueNoiseDepth) * 0x9E3779B9u;
+        // the kernels pick one blue-noise slice per frame, rotated by the golden ratio per pass
+        ap.blue_noise = s->use_gps ? nullptr : s->blue_noise;
         ap.max_fragments = s->max_fragments;
         ap.max_binned = d.max_binned;
         ap.hybrid = s->hybrid_scheduling != 0;
@@ -307,6 +307,7 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     rp.cam = cam;
     rp.spatial_reuse = s->spatial_reuse != 0;
     rp.sh_vec4 = g->sh_bases == 16 && aligned16(g->sh_coefficients);
+    rp.frame_counter = s->frame_index_device;
     rp.temporal_mode = s->temporal_mode;
     err = launch_sample_resolve(rp, stream);
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));

@@ -140,6 +140,12 @@ __global__ void __launch_bounds__(kBlock) sample_kernel(const ResolveParams a) {
     a.reuse_weights[pixel] = weights;
 }
 
+// Advances a device-resident frame index once per call. The last pass of a call does it: every
+// pass that reads the index (accumulate) has finished by then in stream order.
+__device__ __forceinline__ void advance_frame(const ResolveParams& a) {
+    if (a.frame_counter != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.frame_counter += 1u;
+}
+
 __device__ __forceinline__ float3 rgb_to_ycocg(const float3 c) {
     return make_float3(0.25f * c.x + 0.5f * c.y + 0.25f * c.z, 0.5f * c.x - 0.5f * c.z,
                        -0.25f * c.x + 0.5f * c.y - 0.25f * c.z);
@@ -155,6 +161,7 @@ __device__ __forceinline__ float4 catmull_rom_weights(const float t) {
 // then the temporal merge (resolve.cu:164-349).
 template <bool kReuse>
 __global__ void __launch_bounds__(kBlock) resolve_kernel(const ResolveParams a) {
+    advance_frame(a);
     const uint32_t pixel = blockIdx.x * kBlock + threadIdx.x;
     if (pixel >= a.n_pixels) return;
     const uint32_t ss = a.ss;
@@ -339,6 +346,7 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(const ResolveParams a) 
 // box-filters them and merges the history with resolve.cu:191-258's arithmetic. The samples are
 // still written for inspection.
 __global__ void __launch_bounds__(kBlock) sample_resolve_fused_kernel(const ResolveParams a) {
+    advance_frame(a);
     const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
     const bool active = idx < a.n_pixels;
     const uint32_t pixel = active ? idx : a.n_pixels - 1;

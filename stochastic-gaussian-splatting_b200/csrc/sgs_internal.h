@@ -50,16 +50,34 @@ struct AccumulateParams {
     const float4* w2c;
     unsigned long long* framebuffer;
     uint32_t n;
-    uint32_t frame_idx;
+    uint32_t frame_idx;               // used when frame_ptr is null
+    const uint32_t* frame_ptr;        // device-resident frame index, or null
     PassCamera cam;
-    const uint8_t* blue_noise_slice;  // null: white noise
-    uint32_t blue_noise_rotation;
+    const uint8_t* blue_noise;        // (64, 128, 128) volume; null: white noise
     uint32_t max_fragments;           // GPS point cap per Gaussian
     uint32_t max_binned;              // hybrid: binned Gaussian capacity (accumulate_hybrid*.cu max_binned)
     bool hybrid;                      // hybrid scheduling
     WorkQueue* queue;
     QueueArrays q;
 };
+
+// Frame-dependent random-number state of one call: the frame index (from device memory when the
+// caller keeps it there) and the blue-noise slice and rotation it selects (render.cu:77-82).
+struct FrameRng {
+    uint32_t frame;
+    const uint8_t* slice;
+    uint32_t rotation;
+};
+
+__device__ __forceinline__ FrameRng frame_rng(const AccumulateParams& a) {
+    FrameRng r;
+    r.frame = a.frame_ptr != nullptr ? *a.frame_ptr : a.frame_idx;
+    r.slice = a.blue_noise != nullptr
+                  ? a.blue_noise + static_cast<size_t>(r.frame % kBlueNoiseDepth) * kBlueNoiseWidth * kBlueNoiseHeight
+                  : nullptr;
+    r.rotation = (r.frame / kBlueNoiseDepth) * 0x9E3779B9u;
+    return r;
+}
 
 cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue* queue, int num_sms,
                          cudaStream_t stream);
@@ -96,6 +114,7 @@ struct ResolveParams {
     PassCamera cam;                                          // framebuffer (sample)
     bool spatial_reuse;
     bool sh_vec4;    // degree-3 SH at a 16-byte aligned base: winners load their coefficients as float4
+    uint32_t* frame_counter;  // device-resident frame index advanced by the last pass, or null
     int temporal_mode;
 };
 
