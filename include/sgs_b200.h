@@ -137,6 +137,27 @@ int sgs_render(const sgs_gaussians* gaussians, const sgs_camera* camera, const s
 int sgs_render_no_alloc(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
                         const sgs_history* history, const sgs_outputs* outputs, void* stream);
 
+/* Backward pass of stochastic transparency (no counterpart in the reference, which renders only).
+ * Gradients of a loss of the averaged image of S samples w.r.t. means, log-scales, quaternions,
+ * opacity logits and SH coefficients, by an unbiased one-sample estimator of the gradient of the
+ * expected image computed from each sample's winners:
+ *   1. for each sample s, after the sgs_render call that produced it (or a re-render with the same
+ *      frame index and settings), call sgs_backward_accumulate with that call's workspace, the
+ *      upstream gradients of the output image (H, W, 3), alpha and depth (H, W; may be NULL) and
+ *      `weight` = the sample's weight in the averaged output (1/S for a plain progressive average);
+ *      `first` = 1 for the first sample (clears the accumulators);
+ *   2. sgs_backward_finish writes the parameter gradients (overwriting them).
+ * Supported: stochastic transparency (white or blue noise, scatter or hybrid), any supersampling,
+ * Reset/Static; not GPS, spatial reuse or proper antialiasing (SGS_ERROR_INVALID_ARGUMENT).
+ * `backward_workspace` holds sgs_backward_workspace_size(n) bytes, 16-byte aligned. */
+size_t sgs_backward_workspace_size(uint32_t n_gaussians);
+int sgs_backward_accumulate(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                            const void* render_workspace, const float* grad_image, const float* grad_alpha,
+                            const float* grad_depth, float weight, int first, void* backward_workspace, void* stream);
+int sgs_backward_finish(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                        void* backward_workspace, float* d_means, float* d_scales, float* d_rotations,
+                        float* d_opacities, float* d_sh, void* stream);
+
 /* Diagnostics (no counterpart in the reference): CUDA events (cudaEvent_t) that the calling
  * thread's next sgs_render calls record on their stream immediately before the first and after the
  * last kernel of the accumulate stage, so that callers can time that stage with cudaEventElapsedTime.

@@ -144,3 +144,44 @@ def st_uniform(frame: int, g: int, x: int, y: int) -> float:
     h = ((word >> 22) ^ word) & M
     bits = 0x3F800000 | (h >> 9)
     return float(np.array([bits], dtype=np.uint32).view(np.float32)[0]) - 1.0
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None, g_image=None, g_alpha=None,
+                   g_depth=None, grad: bool = False) -> dict:
+    """Expected image of one stochastic-transparency sample (double precision) and, with `grad`, the
+    gradient of sum(g_image * image + g_alpha * alpha + g_depth * depth) w.r.t. every parameter.
+    The fragment support and key order are frozen at `base` (single precision; default: `scene`)."""
+    l = lib()
+    if not hasattr(l.oracle_expected_image, "_typed"):
+        P, u, d, i = _P, ctypes.c_uint32, ctypes.c_double, ctypes.c_int
+        l.oracle_expected_image.argtypes = [P, P, P, P, P, u, u, P, P, u, u, d, d, d, d, d, d, i, P, P, P, P, P, P, P,
+                                            P, P, P, P, P, P, P, P, P]
+        l.oracle_expected_image._typed = True
+    base = scene if base is None else base
+    m, s, r, o, sh = (_f64(scene[k]) for k in ("means", "scales", "rotations", "opacities", "sh_coefficients"))
+    bm, bs, br, bo = (_f32(base[k]) for k in ("means", "scales", "rotations", "opacities"))
+    n, bases = m.shape[0], sh.shape[1]
+    W, H = cam["width"], cam["height"]
+    image = np.zeros((H, W, 3))
+    alpha = np.zeros((H, W, 1))
+    depth = np.zeros((H, W, 1))
+    loss = ctypes.c_double(0.0)
+    gi = None if g_image is None else _f64(g_image)
+    ga = None if g_alpha is None else _f64(g_alpha)
+    gd = None if g_depth is None else _f64(g_depth)
+    out = {}
+    if grad:
+        out = {"means": np.zeros_like(m), "scales": np.zeros_like(s), "rotations": np.zeros_like(r),
+               "opacities": np.zeros_like(o), "sh_coefficients": np.zeros_like(sh)}
+    w2c = _f64(np.asarray(cam["w2c"])[:3].reshape(-1))
+    l.oracle_expected_image(_p(m), _p(s), _p(r), _p(o), _p(sh), n, bases, _p(w2c), _p(_f64(cam["position"])), W, H,
+                            cam["focal_x"], cam["focal_y"], cam["center_x"], cam["center_y"], cam["near_plane"],
+                            cam["far_plane"], int(ss), _p(bm), _p(bs), _p(br), _p(bo), _p(gi), _p(ga), _p(gd),
+                            _p(image), _p(alpha), _p(depth), ctypes.byref(loss),
+                            *(_p(out[k]) if grad else None for k in ("means", "scales", "rotations", "opacities",
+                                                                     "sh_coefficients")))
+    return {"image": image, "alpha": alpha, "depth": depth, "loss": loss.value, "grad": out if grad else None}

@@ -807,3 +807,331 @@ int oracle_fragment_alpha(const float* means, const float* scales, const float* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Expected image of stochastic transparency and its exact gradient (double precision).
+//
+// For a (sub)pixel with fragments i in key order, the expected premultiplied colour, alpha and
+// depth of one sample are C = sum c_i a_i T_i, A = sum a_i T_i, D = sum z_i a_i T_i with
+// T_i = prod_{j before i} (1 - a_j). The fragment support (which Gaussian reaches which pixel with
+// alpha >= 1/255) and the key order are frozen at a base point given in single precision (the
+// forward of the render path); within them the image is a smooth function of the parameters, whose
+// derivative is what a gradient estimator must reproduce on average. This is the checker of the
+// backward pass: no reference counterpart exists (the reference has no backward).
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+struct ProjD {
+    double t[3], x, y, xc, yc;
+    bool free_x, free_y;
+    double qn[4], qnorm;
+    double R[3][3], v[3], S[3][3], T[2][3];
+    double a, b, c, det, conic[3];
+    double op, m2[2];
+    double dvec[3], dlen, dir[3], color[3], Y[16];
+    bool cpos[3];
+};
+
+constexpr double kC0 = 0.28209479177387814, kC1 = 0.48860251190291987, kC2a = 1.0925484305920792,
+                 kC2b = 0.94617469575755997, kC2c = 0.31539156525251999, kC2d = 0.54627421529603959,
+                 kC3a = 0.59004358992664352, kC3b = 1.7701307697799304, kC3c = 2.8906114426405538,
+                 kC3d = 0.45704579946446572, kC3e = 2.2852289973223288, kC3f = 1.865881662950577,
+                 kC3g = 1.1195289977703462, kC3h = 1.4453057213202769;
+
+// signed SH basis of the reference's eval_sh (gs_utils.h:212-243) and its gradient w.r.t. the direction
+void sh_basis(const double x, const double y, const double z, double Y[16], double dY[16][3]) {
+    const double xx = x * x, yy = y * y, zz = z * z;
+    double v[16] = {kC0, -kC1 * y, kC1 * z, -kC1 * x, kC2a * x * y, -kC2a * y * z, kC2b * zz - kC2c, -kC2a * x * z,
+                    kC2d * (xx - yy), y * (kC3a * yy - kC3b * xx), kC3c * x * y * z, y * (kC3d - kC3e * zz),
+                    z * (kC3f * zz - kC3g), x * (kC3d - kC3e * zz), kC3h * z * (xx - yy), x * (kC3b * yy - kC3a * xx)};
+    double g[16][3] = {{0, 0, 0}, {0, -kC1, 0}, {0, 0, kC1}, {-kC1, 0, 0},
+                       {kC2a * y, kC2a * x, 0}, {0, -kC2a * z, -kC2a * y}, {0, 0, 2 * kC2b * z},
+                       {-kC2a * z, 0, -kC2a * x}, {2 * kC2d * x, -2 * kC2d * y, 0},
+                       {-2 * kC3b * x * y, 3 * kC3a * yy - kC3b * xx, 0}, {kC3c * y * z, kC3c * x * z, kC3c * x * y},
+                       {0, kC3d - kC3e * zz, -2 * kC3e * y * z}, {0, 0, 3 * kC3f * zz - kC3g},
+                       {kC3d - kC3e * zz, 0, -2 * kC3e * x * z}, {2 * kC3h * x * z, -2 * kC3h * y * z, kC3h * (xx - yy)},
+                       {kC3b * yy - 3 * kC3a * xx, 2 * kC3b * x * y, 0}};
+    std::memcpy(Y, v, sizeof(v));
+    std::memcpy(dY, g, sizeof(g));
+}
+
+ProjD project_d(const double* m, const double* s, const double* q, const double o, const double* sh, uint32_t bases,
+                const double* W, const double* cam, const double fx, const double fy, const double cx0,
+                const double cy0, const double width, const double height, const double dil) {
+    ProjD p{};
+    for (int r = 0; r < 3; ++r) p.t[r] = W[4 * r] * m[0] + W[4 * r + 1] * m[1] + W[4 * r + 2] * m[2] + W[4 * r + 3];
+    p.x = p.t[0] / p.t[2];
+    p.y = p.t[1] / p.t[2];
+    const double cl = (-0.15 * width - cx0) / fx, cr = (1.15 * width - cx0) / fx;
+    const double ct = (-0.15 * height - cy0) / fy, cb = (1.15 * height - cy0) / fy;
+    p.xc = std::min(std::max(p.x, cl), cr);
+    p.yc = std::min(std::max(p.y, ct), cb);
+    p.free_x = p.x > cl && p.x < cr;
+    p.free_y = p.y > ct && p.y < cb;
+    p.qnorm = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (int i = 0; i < 4; ++i) p.qn[i] = q[i] / p.qnorm;
+    const double w = p.qn[0], X = p.qn[1], Yq = p.qn[2], Z = p.qn[3];
+    const double R[3][3] = {{1 - 2 * (Yq * Yq + Z * Z), 2 * (X * Yq - w * Z), 2 * (X * Z + w * Yq)},
+                            {2 * (X * Yq + w * Z), 1 - 2 * (X * X + Z * Z), 2 * (Yq * Z - w * X)},
+                            {2 * (X * Z - w * Yq), 2 * (Yq * Z + w * X), 1 - 2 * (X * X + Yq * Yq)}};
+    std::memcpy(p.R, R, sizeof(R));
+    for (int i = 0; i < 3; ++i) p.v[i] = std::exp(2.0 * s[i]);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 3; ++k) acc += R[i][k] * p.v[k] * R[j][k];
+            p.S[i][j] = acc;
+        }
+    const double J[2][3] = {{fx / p.t[2], 0, -fx * p.xc / p.t[2]}, {0, fy / p.t[2], -fy * p.yc / p.t[2]}};
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 3; ++k) acc += J[i][k] * W[4 * k + j];
+            p.T[i][j] = acc;
+        }
+    double cov[2][2];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l) acc += p.T[i][k] * p.S[k][l] * p.T[j][l];
+            cov[i][j] = acc;
+        }
+    p.a = cov[0][0] + dil;
+    p.b = cov[0][1];
+    p.c = cov[1][1] + dil;
+    p.det = p.a * p.c - p.b * p.b;
+    p.conic[0] = p.c / p.det;
+    p.conic[1] = -p.b / p.det;
+    p.conic[2] = p.a / p.det;
+    p.op = 1.0 / (1.0 + std::exp(-o));
+    p.m2[0] = p.x * fx + cx0;
+    p.m2[1] = p.y * fy + cy0;
+    for (int i = 0; i < 3; ++i) p.dvec[i] = m[i] - cam[i];
+    p.dlen = std::sqrt(p.dvec[0] * p.dvec[0] + p.dvec[1] * p.dvec[1] + p.dvec[2] * p.dvec[2]);
+    for (int i = 0; i < 3; ++i) p.dir[i] = p.dvec[i] / p.dlen;
+    double dY[16][3];
+    sh_basis(p.dir[0], p.dir[1], p.dir[2], p.Y, dY);
+    for (int ch = 0; ch < 3; ++ch) {
+        double col = 0.5;
+        for (uint32_t bb = 0; bb < bases; ++bb) col += p.Y[bb] * sh[3 * bb + ch];
+        p.cpos[ch] = col > 0.0;
+        p.color[ch] = std::max(col, 0.0);
+    }
+    return p;
+}
+
+// upstream gradients of one Gaussian's projected quantities
+struct GradProj {
+    double op, conic[3], m2[2], depth, color[3];
+};
+
+// chain rule from the projected quantities to the parameters (mean, log-scale, quaternion, logit, SH)
+void project_d_backward(const ProjD& p, const GradProj& g, const double* sh, uint32_t bases, const double* W,
+                        const double fx, const double fy, double* dm, double* ds, double* dq, double* dopac,
+                        double* dsh) {
+    *dopac = g.op * p.op * (1.0 - p.op);
+    // conic = inverse(cov2d + dilation): dL/dcov = -C G C
+    const double C[2][2] = {{p.conic[0], p.conic[1]}, {p.conic[1], p.conic[2]}};
+    const double G[2][2] = {{g.conic[0], 0.5 * g.conic[1]}, {0.5 * g.conic[1], g.conic[2]}};
+    double CG[2][2], GA[2][2];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) CG[i][j] = C[i][0] * G[0][j] + C[i][1] * G[1][j];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) GA[i][j] = -(CG[i][0] * C[0][j] + CG[i][1] * C[1][j]);
+    // G_cov symmetric with off-diagonal dL/db / 2 = GA[0][1]
+    double dS[3][3], dT[2][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 2; ++k)
+                for (int l = 0; l < 2; ++l) acc += p.T[k][i] * GA[k][l] * p.T[l][j];
+            dS[i][j] = acc;
+        }
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 2; ++k)
+                for (int l = 0; l < 3; ++l) acc += GA[i][k] * p.T[k][l] * p.S[l][j];
+            dT[i][j] = 2.0 * acc;
+        }
+    // T = J W3
+    double dJ[2][3];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 3; ++k) acc += dT[i][k] * W[4 * j + k];
+            dJ[i][j] = acc;
+        }
+    const double tz = p.t[2];
+    double dtx = 0, dty = 0, dtz = g.depth;
+    dtz += dJ[0][0] * (-fx / (tz * tz)) + dJ[0][2] * (fx * p.xc / (tz * tz)) + dJ[1][1] * (-fy / (tz * tz)) +
+           dJ[1][2] * (fy * p.yc / (tz * tz));
+    double dx = g.m2[0] * fx, dy = g.m2[1] * fy;
+    if (p.free_x) dx += dJ[0][2] * (-fx / tz);
+    if (p.free_y) dy += dJ[1][2] * (-fy / tz);
+    dtx += dx / tz;
+    dty += dy / tz;
+    dtz -= dx * p.t[0] / (tz * tz) + dy * p.t[1] / (tz * tz);
+    for (int i = 0; i < 3; ++i) dm[i] = W[i] * dtx + W[4 + i] * dty + W[8 + i] * dtz;
+    // Sigma = R V R^T
+    for (int i = 0; i < 3; ++i) {
+        double acc = 0;
+        for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) acc += p.R[k][i] * dS[k][l] * p.R[l][i];
+        ds[i] = acc * 2.0 * p.v[i];
+    }
+    double dR[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0;
+            for (int k = 0; k < 3; ++k) acc += (dS[i][k] + dS[k][i]) * p.R[k][j];
+            dR[i][j] = acc * p.v[j];
+        }
+    const double w = p.qn[0], X = p.qn[1], Y = p.qn[2], Z = p.qn[3];
+    double dqn[4];
+    dqn[0] = 2 * (-Z * dR[0][1] + Y * dR[0][2] + Z * dR[1][0] - X * dR[1][2] - Y * dR[2][0] + X * dR[2][1]);
+    dqn[1] = 2 * (Y * dR[0][1] + Z * dR[0][2] + Y * dR[1][0] - 2 * X * dR[1][1] - w * dR[1][2] + Z * dR[2][0] +
+                  w * dR[2][1] - 2 * X * dR[2][2]);
+    dqn[2] = 2 * (-2 * Y * dR[0][0] + X * dR[0][1] + w * dR[0][2] + X * dR[1][0] + Z * dR[1][2] - w * dR[2][0] +
+                  Z * dR[2][1] - 2 * Y * dR[2][2]);
+    dqn[3] = 2 * (-2 * Z * dR[0][0] - w * dR[0][1] + X * dR[0][2] + w * dR[1][0] - 2 * Z * dR[1][1] + Y * dR[1][2] +
+                  X * dR[2][0] + Y * dR[2][1]);
+    const double dot = dqn[0] * w + dqn[1] * X + dqn[2] * Y + dqn[3] * Z;
+    for (int i = 0; i < 4; ++i) dq[i] = (dqn[i] - p.qn[i] * dot) / p.qnorm;
+    // colour = max(0.5 + sum Y_b sh_b, 0) per channel; direction = normalize(mean - camera)
+    double Yb[16], dY[16][3];
+    sh_basis(p.dir[0], p.dir[1], p.dir[2], Yb, dY);
+    double ddir[3] = {0, 0, 0};
+    for (int ch = 0; ch < 3; ++ch) {
+        const double gc = p.cpos[ch] ? g.color[ch] : 0.0;
+        for (uint32_t bb = 0; bb < bases; ++bb) {
+            dsh[3 * bb + ch] = gc * Yb[bb];
+            for (int k = 0; k < 3; ++k) ddir[k] += gc * sh[3 * bb + ch] * dY[bb][k];
+        }
+    }
+    const double dd = ddir[0] * p.dir[0] + ddir[1] * p.dir[1] + ddir[2] * p.dir[2];
+    for (int k = 0; k < 3; ++k) dm[k] += (ddir[k] - p.dir[k] * dd) / p.dlen;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Expected image (H, W, 3 / 1 / 1) of one stochastic-transparency sample, image resolution (the
+// ss x ss box filter applied), and the gradient of L = sum(g_image * image + g_alpha * alpha +
+// g_depth * depth) w.r.t. every parameter. Support and key order come from the single-precision
+// projection of the `base_*` parameters; `d_*` may be null for the forward only.
+int oracle_expected_image(const double* means, const double* scales, const double* rotations, const double* opacities,
+                          const double* sh, uint32_t n, uint32_t bases, const double* w2c, const double* cam_pos,
+                          uint32_t width, uint32_t height, double fx, double fy, double cx, double cy, double near_plane,
+                          double far_plane, int ss_raw, const float* base_means, const float* base_scales,
+                          const float* base_rotations, const float* base_opacities, const double* g_image,
+                          const double* g_alpha, const double* g_depth, double* image, double* alpha, double* depth,
+                          double* loss, double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
+                          double* d_sh) {
+    const uint32_t ss = ss_raw < 1 ? 1u : static_cast<uint32_t>(ss_raw);
+    float w2cf[12];
+    for (int i = 0; i < 12; ++i) w2cf[i] = static_cast<float>(w2c[i]);
+    const Cam cam = make_cam(width, height, static_cast<float>(fx), static_cast<float>(fy), static_cast<float>(cx),
+                             static_cast<float>(cy), static_cast<float>(near_plane), static_cast<float>(far_plane), 0,
+                             static_cast<int>(ss));
+    const uint32_t fbw = width * ss, fbh = height * ss;
+    const double dfx = fx * ss, dfy = fy * ss, dcx = cx * ss, dcy = cy * ss;
+    const double dil = kDilation * ss * ss;
+    // frozen support and order from the single-precision forward
+    std::vector<std::vector<std::pair<uint64_t, uint32_t>>> frags(static_cast<size_t>(fbw) * fbh);
+    for (uint32_t g = 0; g < n; ++g) {
+        const Proj p = project(base_means, base_scales, base_rotations, base_opacities, w2cf, g, cam);
+        if (!p.active) continue;
+        const Rect rc = rect_of(p, cam);
+        const uint64_t key = pack(p.depth, g);
+        for (uint32_t yy = 0; yy < rc.h; ++yy)
+            for (uint32_t xx = 0; xx < rc.w; ++xx) {
+                const uint32_t px = rc.x0 + xx, py = rc.y0 + yy;
+                if (st_alpha(p, static_cast<float>(px), static_cast<float>(py), false) < kMinAlpha) continue;
+                frags[static_cast<size_t>(py) * fbw + px].push_back({key, g});
+            }
+    }
+    std::vector<ProjD> pd(n);
+    for (uint32_t g = 0; g < n; ++g)
+        pd[g] = project_d(means + 3 * g, scales + 3 * g, rotations + 4 * g, opacities[g], sh + static_cast<size_t>(g) * bases * 3,
+                          bases, w2c, cam_pos, dfx, dfy, dcx, dcy, static_cast<double>(fbw), static_cast<double>(fbh), dil);
+    const bool grad = d_means != nullptr;
+    std::vector<GradProj> gp(grad ? n : 0);
+    for (auto& x : gp) x = GradProj{};
+    const double norm = 1.0 / (ss * ss);
+    const size_t n_px = static_cast<size_t>(width) * height;
+    std::fill(image, image + 3 * n_px, 0.0);
+    std::fill(alpha, alpha + n_px, 0.0);
+    std::fill(depth, depth + n_px, 0.0);
+    double L = 0.0;
+    std::vector<double> al, ci, suffix_c, suffix_z;
+    for (uint32_t py = 0; py < fbh; ++py)
+        for (uint32_t px = 0; px < fbw; ++px) {
+            auto& f = frags[static_cast<size_t>(py) * fbw + px];
+            std::sort(f.begin(), f.end());
+            const size_t ip = static_cast<size_t>(py / ss) * width + px / ss;
+            const size_t m = f.size();
+            al.assign(m, 0.0);
+            std::vector<double> T(m + 1, 1.0);
+            for (size_t k = 0; k < m; ++k) {
+                const ProjD& p = pd[f[k].second];
+                const double dx = px - (p.m2[0] - 0.5), dy = py - (p.m2[1] - 0.5);
+                const double e = -0.5 * (p.conic[0] * dx * dx + p.conic[2] * dy * dy) - p.conic[1] * dx * dy;
+                al[k] = p.op * std::exp(std::min(e, 0.0));
+                T[k + 1] = T[k] * (1.0 - al[k]);
+            }
+            double Cc[3] = {0, 0, 0}, Aa = 0, Dd = 0;
+            for (size_t k = 0; k < m; ++k) {
+                const ProjD& p = pd[f[k].second];
+                const double wgt = al[k] * T[k];
+                for (int ch = 0; ch < 3; ++ch) Cc[ch] += p.color[ch] * wgt;
+                Aa += wgt;
+                Dd += p.t[2] * wgt;
+            }
+            for (int ch = 0; ch < 3; ++ch) image[3 * ip + ch] += Cc[ch] * norm;
+            alpha[ip] += Aa * norm;
+            depth[ip] += Dd * norm;
+            if (g_image == nullptr) continue;
+            const double gi[3] = {g_image[3 * ip] * norm, g_image[3 * ip + 1] * norm, g_image[3 * ip + 2] * norm};
+            const double ga = g_alpha ? g_alpha[ip] * norm : 0.0, gdp = g_depth ? g_depth[ip] * norm : 0.0;
+            L += gi[0] * Cc[0] + gi[1] * Cc[1] + gi[2] * Cc[2] + ga * Aa + gdp * Dd;
+            if (!grad) continue;
+            // suffix sums over the fragments behind k
+            double sc = 0.0, sz = 0.0;
+            for (size_t kk = m; kk-- > 0;) {
+                const uint32_t g = f[kk].second;
+                const ProjD& p = pd[g];
+                const double a = al[kk];
+                double gc = 0.0;
+                for (int ch = 0; ch < 3; ++ch) gc += gi[ch] * p.color[ch];
+                const double inv = 1.0 / std::max(1.0 - a, 1e-12);
+                const double dA = gc * T[kk] - sc * inv + ga * T[m] * inv + gdp * (p.t[2] * T[kk] - sz * inv);
+                double gcol = 0.0;
+                for (int ch = 0; ch < 3; ++ch) gcol += gi[ch] * p.color[ch];
+                sc += gcol * a * T[kk];
+                sz += p.t[2] * a * T[kk];
+                GradProj& G = gp[g];
+                for (int ch = 0; ch < 3; ++ch) G.color[ch] += gi[ch] * a * T[kk];
+                G.depth += gdp * a * T[kk];
+                // a = op * exp(e), e = -0.5 (cX dx^2 + cZ dy^2) - cY dx dy, dx = px - (m2x - 0.5)
+                const double dx = px - (p.m2[0] - 0.5), dy = py - (p.m2[1] - 0.5);
+                const double dAe = dA * a;
+                G.op += dA * (a / p.op);
+                G.conic[0] += dAe * (-0.5 * dx * dx);
+                G.conic[1] += dAe * (-dx * dy);
+                G.conic[2] += dAe * (-0.5 * dy * dy);
+                G.m2[0] += dAe * (p.conic[0] * dx + p.conic[1] * dy);
+                G.m2[1] += dAe * (p.conic[1] * dx + p.conic[2] * dy);
+            }
+        }
+    if (loss) *loss = L;
+    if (!grad) return 0;
+    for (uint32_t g = 0; g < n; ++g)
+        project_d_backward(pd[g], gp[g], sh + static_cast<size_t>(g) * bases * 3, bases, w2c, dfx, dfy, d_means + 3 * g,
+                           d_scales + 3 * g, d_rotations + 4 * g, d_opacities + g, d_sh + static_cast<size_t>(g) * bases * 3);
+    return 0;
+}
+
+}  // extern "C"

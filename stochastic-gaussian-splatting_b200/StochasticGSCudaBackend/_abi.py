@@ -101,6 +101,15 @@ SIGNATURES = {
     "sgs_render_no_alloc": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
                                            ctypes.POINTER(SettingsC), ctypes.POINTER(HistoryC),
                                            ctypes.POINTER(Outputs), ctypes.c_void_p]),
+    "sgs_backward_workspace_size": (ctypes.c_size_t, [ctypes.c_uint32]),
+    "sgs_backward_accumulate": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
+                                               ctypes.POINTER(SettingsC), ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_int,
+                                               ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_backward_finish": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
+                                           ctypes.POINTER(SettingsC), ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
     "sgs_set_stage_events": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_get_frame_index": (ctypes.c_uint32, []),
     "sgs_set_frame_index": (None, [ctypes.c_uint32]),

@@ -1,0 +1,117 @@
+"""Differentiable rendering: gradients of the progressively averaged image w.r.t. the Gaussians.
+
+`render_samples(means, scales, rotations, opacities, sh, settings, n_samples)` renders n_samples
+stochastic-transparency samples (Reset, then Static: their plain average, as Renderer.py's
+SAMPLES_PER_PIXEL loop produces it) and returns (image, depth, alpha) like `History`, with a
+backward pass to all five parameter tensors (the reference renders only; it has no backward).
+
+The backward is an unbiased estimator of the gradient of the expected image (see
+csrc/backward_st.cu): each sample's winners give a one-sample estimate, averaged over the samples.
+Winners are either kept from the forward pass (`store_winners=True`, 24 bytes per framebuffer pixel
+and sample) or recomputed by rendering the same frame indices again (`store_winners=False`: no
+memory per sample, one more render per sample).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _abi, _C
+from .render import Settings
+
+_lib = _abi.load()
+
+
+def _structs(means, scales, rotations, opacities, sh, settings: Settings):
+    g = _abi.Gaussians(means.data_ptr(), scales.data_ptr(), rotations.data_ptr(), opacities.data_ptr(), sh.data_ptr(),
+                       means.shape[0], sh.shape[1])
+    c = _abi.Camera(settings.w2c.data_ptr(), settings.cam_position.data_ptr(), settings.width, settings.height,
+                    float(settings.focal_x), float(settings.focal_y), float(settings.center_x),
+                    float(settings.center_y), float(settings.near_plane), float(settings.far_plane))
+    s = _abi.SettingsC(int(settings.proper_antialiasing), max(1, int(settings.supersampling_factor)),
+                       int(settings.use_gps), int(settings.hybrid_scheduling), int(settings.spatial_reuse), 1, None,
+                       None, 0, 0, None)
+    return g, c, s
+
+
+def _render_one(tensors, settings: Settings, hist, mode: int, frame: int):
+    _C.set_frame_index(frame)
+    n_fb = settings.width * settings.height * max(1, settings.supersampling_factor) ** 2
+    dev = tensors[0].device
+    kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device=dev), torch.empty((0, n_fb, 4), device=dev))
+    return _C.render_with_workspace(*tensors, *settings.as_tuple(), torch.empty(0, dtype=torch.uint8, device=dev),
+                                    *kb, *hist, torch.eye(4, device=dev), mode)
+
+
+class _RenderSamples(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, means, scales, rotations, opacities, sh, settings, n_samples, first_frame, store_winners):
+        if settings.use_gps or settings.spatial_reuse or settings.proper_antialiasing:
+            raise RuntimeError("render_samples differentiates stochastic transparency without spatial reuse or "
+                               "proper antialiasing")
+        tensors = tuple(t.detach().contiguous() for t in (means, scales, rotations, opacities, sh))
+        e = torch.empty(0)
+        hist = (e, e, e, e)
+        workspaces = []
+        for s in range(n_samples):
+            outs, ws, _ = _render_one(tensors, settings, hist, 0 if s == 0 else 1, first_frame + s)
+            hist = outs
+            if store_winners:
+                workspaces.append(ws)
+        ctx.save_for_backward(*tensors)
+        ctx.settings = settings
+        ctx.n_samples = n_samples
+        ctx.first_frame = first_frame
+        ctx.workspaces = workspaces
+        image, depth, alpha, _ = hist
+        return image, depth, alpha
+
+    @staticmethod
+    def backward(ctx, g_image, g_depth, g_alpha):
+        tensors = ctx.saved_tensors
+        settings = ctx.settings
+        dev = tensors[0].device
+        g, c, s = _structs(*tensors, settings)
+        grads_in = [None if t is None else t.contiguous() for t in (g_image, g_alpha, g_depth)]
+        if grads_in[0] is None:
+            grads_in[0] = torch.zeros((settings.height, settings.width, 3), device=dev)
+        bw = torch.empty(_lib.sgs_backward_workspace_size(tensors[0].shape[0]) // 4 + 4, dtype=torch.float32,
+                         device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        weight = 1.0 / ctx.n_samples
+        e = torch.empty(0)
+        hist = (e, e, e, e)
+        for k in range(ctx.n_samples):
+            if ctx.workspaces:
+                ws = ctx.workspaces[k]
+            else:
+                hist, ws, _ = _render_one(tensors, settings, hist, 0 if k == 0 else 1, ctx.first_frame + k)
+            st = _lib.sgs_backward_accumulate(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
+                                              ctypes.c_void_p(ws.data_ptr()), ctypes.c_void_p(grads_in[0].data_ptr()),
+                                              None if grads_in[1] is None else ctypes.c_void_p(grads_in[1].data_ptr()),
+                                              None if grads_in[2] is None else ctypes.c_void_p(grads_in[2].data_ptr()),
+                                              ctypes.c_float(weight), int(k == 0), ctypes.c_void_p(bw.data_ptr()),
+                                              ctypes.c_void_p(stream))
+            if st != _abi.SGS_OK:
+                raise RuntimeError(f"sgs_backward_accumulate failed ({st}): {_abi.last_error(_lib)}")
+        outs = [torch.empty_like(t) for t in tensors]
+        st = _lib.sgs_backward_finish(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(bw.data_ptr()),
+                                      *(ctypes.c_void_p(t.data_ptr()) for t in outs), ctypes.c_void_p(stream))
+        if st != _abi.SGS_OK:
+            raise RuntimeError(f"sgs_backward_finish failed ({st}): {_abi.last_error(_lib)}")
+        ctx.workspaces = []
+        return (*outs, None, None, None, None)
+
+
+def render_samples(means, scales, rotations, opacities, sh_coefficients, settings: Settings, n_samples: int = 1,
+                   first_frame: int | None = None, store_winners: bool = True):
+    """Differentiable average of `n_samples` stochastic-transparency samples: (image, depth, alpha),
+    premultiplied by alpha like `History`. Frames first_frame .. first_frame + n_samples - 1 (default:
+    the process-wide frame index, which advances by n_samples)."""
+    if first_frame is None:
+        first_frame = _C.get_frame_index()
+    out = _RenderSamples.apply(means, scales, rotations, opacities, sh_coefficients, settings, int(n_samples),
+                               int(first_frame), bool(store_winners))
+    _C.set_frame_index(first_frame + n_samples)
+    return out

@@ -1,0 +1,332 @@
+// Backward pass of stochastic transparency: an unbiased one-sample estimator of the gradient of the
+// expected image, computed from the sample's own winners (the reference has no backward).
+//
+// For a (sub)pixel with fragments in key order, one sample's colour, alpha and depth have the
+// expectations C = sum c_i a_i T_i, A = sum a_i T_i, D = sum z_i a_i T_i (T_i = prod over the
+// fragments before i of (1 - a_j)). With w the sample's winner (the closest accepted fragment):
+//   E[1(w = k)]            = a_k T_k                  -> dC/dc_k, dD/dz_k
+//   E[1(key_w >= key_k)]   = T_k                      (nothing before k was accepted)
+//   E[1(key_w >  key_k) c_w] = sum_{i after k} c_i a_i T_i
+//   E[1(w = none)]         = 1 - A
+// so that, per sample, with upstream gradients g (colour), g_a, g_d of the pixel,
+//   dL/da_k ~ g.(1(key_w >= key_k) c_k - 1(key_w > key_k) c_w / (1 - a_k))
+//           + g_a 1(w = none) / (1 - a_k) + g_d (1(key_w >= key_k) z_k - 1(key_w > key_k) z_w / (1 - a_k))
+// is unbiased for dE[L]/da_k of a linear loss. Fragment gradients are accumulated per Gaussian in
+// its projected quantities (opacity, conic, 2-D mean, depth, colour) and a projection backward
+// chains them to means, log-scales, quaternions, opacity logits and SH coefficients. The winners
+// come from re-rendering the sample (same frame index) or from its stored framebuffer.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "sgs_internal.h"
+
+namespace sgs {
+namespace {
+
+constexpr uint32_t kBlock = 256;
+constexpr uint32_t kFullMask = 0xffffffffu;
+constexpr uint32_t kCoopFragments = 64;  // larger AABBs are processed by the whole warp
+constexpr int kAccum = 10;               // op, conic x/y/z, mean2d x/y, depth, colour r/g/b
+
+// View-dependent colour of every Gaussian (the colour its fragments would give a pixel).
+__global__ void __launch_bounds__(kBlock) colors_kernel(const BackwardParams b) {
+    const uint32_t g = blockIdx.x * kBlock + threadIdx.x;
+    if (g >= b.n) return;
+    const float vx = b.means[3 * g + 0] - b.cam_position[0];
+    const float vy = b.means[3 * g + 1] - b.cam_position[1];
+    const float vz = b.means[3 * g + 2] - b.cam_position[2];
+    const float inv_len = rsqrtf(vx * vx + vy * vy + vz * vz);
+    const float3 c = eval_sh(b.sh + static_cast<size_t>(g) * b.sh_bases * 3, vx * inv_len, vy * inv_len, vz * inv_len,
+                             b.sh_bases);
+    b.colors[3 * g + 0] = c.x;
+    b.colors[3 * g + 1] = c.y;
+    b.colors[3 * g + 2] = c.z;
+}
+
+struct FragAccum {
+    float v[kAccum];
+};
+
+// Contribution of one fragment of Gaussian k at framebuffer pixel (px, py) to k's accumulators.
+__device__ __forceinline__ void fragment_grad(const BackwardParams& b, const Projected& p, const float3 ce,
+                                             const unsigned long long key_k, const float3 ck, const uint32_t px,
+                                             const uint32_t py, FragAccum& acc) {
+    const float mx = p.mean2d.x - 0.5f, my = p.mean2d.y - 0.5f;
+    const float dx = static_cast<float>(px) - mx;
+    const float dy = static_cast<float>(py) - my;
+    const float alpha = fragment_alpha(ce, p.opacity, dx, dy);
+    if (alpha < kMinAlpha) return;
+    const uint32_t pix = py * b.cam.width_int + px;
+    const unsigned long long key_w = b.framebuffer[pix];
+    const float4 sw = b.samples[pix];  // winner colour and depth (0 for background)
+    // upstream gradients of the image pixel, spread over its subpixels and the averaged samples
+    const uint32_t ip = (py / b.ss) * b.width + px / b.ss;
+    const float gs = b.grad_scale;
+    const float g0 = b.grad_image[3 * ip + 0] * gs, g1 = b.grad_image[3 * ip + 1] * gs, g2 = b.grad_image[3 * ip + 2] * gs;
+    const float ga = b.grad_alpha != nullptr ? b.grad_alpha[ip] * gs : 0.0f;
+    const float gd = b.grad_depth != nullptr ? b.grad_depth[ip] * gs : 0.0f;
+    const bool ge = key_w >= key_k;
+    const bool gt = key_w > key_k;
+    const bool none = key_w == kEmptyFragment;
+    const float inv = 1.0f / fmaxf(1.0f - alpha, 1e-12f);
+    const float gck = g0 * ck.x + g1 * ck.y + g2 * ck.z;
+    const float gcw = g0 * sw.x + g1 * sw.y + g2 * sw.z;
+    float dA = (ge ? gck : 0.0f) - (gt ? gcw * inv : 0.0f) + (none ? ga * inv : 0.0f);
+    dA += gd * ((ge ? p.depth : 0.0f) - (gt ? sw.w * inv : 0.0f));
+    if (key_w == key_k) {  // this Gaussian won the pixel
+        acc.v[6] += gd;
+        acc.v[7] += g0;
+        acc.v[8] += g1;
+        acc.v[9] += g2;
+    }
+    // alpha = opacity exp(-0.5 (cX dx^2 + cZ dy^2) - cY dx dy)
+    const float dAe = dA * alpha;
+    acc.v[0] += dA * (alpha / p.opacity);
+    acc.v[1] += dAe * (-0.5f * dx * dx);
+    acc.v[2] += dAe * (-dx * dy);
+    acc.v[3] += dAe * (-0.5f * dy * dy);
+    acc.v[4] += dAe * (p.conic.x * dx + p.conic.y * dy);
+    acc.v[5] += dAe * (p.conic.y * dx + p.conic.z * dy);
+}
+
+// One thread per Gaussian; AABBs above kCoopFragments pixels are processed by the whole warp.
+__global__ void __launch_bounds__(kBlock) fragments_backward_kernel(const BackwardParams b) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
+    bool active = idx < b.n;
+    const uint32_t g = active ? idx : b.n - 1;
+    Projected p;
+    if (!project_gaussian(active, g, b.means, b.scales, b.rotations, b.opacities, b.w2c, b.cam, p)) return;
+    const PixelRect rect = pixel_rect(p.bounds, b.cam);
+    const uint32_t count = active ? rect.width * rect.height : 0u;
+    const float3 ce = conic_for_exp2(p.conic);
+    const unsigned long long key = pack_fragment(p.depth, g);
+    const float3 ck = make_float3(b.colors[3 * g + 0], b.colors[3 * g + 1], b.colors[3 * g + 2]);
+    FragAccum acc;
+#pragma unroll
+    for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
+    if (count <= kCoopFragments) {
+        for (uint32_t f = 0; f < count; ++f)
+            fragment_grad(b, p, ce, key, ck, rect.x_min + f % rect.width, rect.y_min + f / rect.width, acc);
+    }
+    uint32_t pending = __ballot_sync(kFullMask, count > kCoopFragments);
+    while (pending) {
+        const uint32_t src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        Projected q;
+        q.depth = __shfl_sync(kFullMask, p.depth, src);
+        q.opacity = __shfl_sync(kFullMask, p.opacity, src);
+        q.mean2d = make_float2(__shfl_sync(kFullMask, p.mean2d.x, src), __shfl_sync(kFullMask, p.mean2d.y, src));
+        q.conic = make_float3(__shfl_sync(kFullMask, p.conic.x, src), __shfl_sync(kFullMask, p.conic.y, src),
+                              __shfl_sync(kFullMask, p.conic.z, src));
+        const float3 qce = conic_for_exp2(q.conic);
+        const unsigned long long qkey = __shfl_sync(kFullMask, key, src);
+        const float3 qck = make_float3(__shfl_sync(kFullMask, ck.x, src), __shfl_sync(kFullMask, ck.y, src),
+                                       __shfl_sync(kFullMask, ck.z, src));
+        const uint32_t x0 = __shfl_sync(kFullMask, rect.x_min, src), y0 = __shfl_sync(kFullMask, rect.y_min, src);
+        const uint32_t w = __shfl_sync(kFullMask, rect.width, src), n = __shfl_sync(kFullMask, count, src);
+        FragAccum part;
+#pragma unroll
+        for (int i = 0; i < kAccum; ++i) part.v[i] = 0.0f;
+        for (uint32_t f = lane; f < n; f += 32) fragment_grad(b, q, qce, qkey, qck, x0 + f % w, y0 + f / w, part);
+#pragma unroll
+        for (int i = 0; i < kAccum; ++i) {
+            float v = part.v[i];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+            if (lane == src) acc.v[i] += v;
+        }
+    }
+    if (!active) return;
+    float* out = b.accum + static_cast<size_t>(g) * kAccum;
+#pragma unroll
+    for (int i = 0; i < kAccum; ++i)
+        if (acc.v[i] != 0.0f) out[i] += acc.v[i];
+}
+
+// Signed SH basis of eval_sh (gs_utils.h:212-243) and its gradient w.r.t. the direction.
+__device__ __forceinline__ void sh_basis(const float x, const float y, const float z, float Y[16], float dY[16][3]) {
+    const float xx = x * x, yy = y * y, zz = z * z;
+    Y[0] = kSH0; dY[0][0] = 0; dY[0][1] = 0; dY[0][2] = 0;
+    Y[1] = -kSH1 * y; dY[1][0] = 0; dY[1][1] = -kSH1; dY[1][2] = 0;
+    Y[2] = kSH1 * z; dY[2][0] = 0; dY[2][1] = 0; dY[2][2] = kSH1;
+    Y[3] = -kSH1 * x; dY[3][0] = -kSH1; dY[3][1] = 0; dY[3][2] = 0;
+    Y[4] = kSH2a * x * y; dY[4][0] = kSH2a * y; dY[4][1] = kSH2a * x; dY[4][2] = 0;
+    Y[5] = -kSH2a * y * z; dY[5][0] = 0; dY[5][1] = -kSH2a * z; dY[5][2] = -kSH2a * y;
+    Y[6] = kSH2b * zz - kSH2c; dY[6][0] = 0; dY[6][1] = 0; dY[6][2] = 2.0f * kSH2b * z;
+    Y[7] = -kSH2a * x * z; dY[7][0] = -kSH2a * z; dY[7][1] = 0; dY[7][2] = -kSH2a * x;
+    Y[8] = kSH2d * (xx - yy); dY[8][0] = 2.0f * kSH2d * x; dY[8][1] = -2.0f * kSH2d * y; dY[8][2] = 0;
+    Y[9] = y * (kSH3a * yy - kSH3b * xx); dY[9][0] = -2.0f * kSH3b * x * y; dY[9][1] = 3.0f * kSH3a * yy - kSH3b * xx; dY[9][2] = 0;
+    Y[10] = kSH3c * x * y * z; dY[10][0] = kSH3c * y * z; dY[10][1] = kSH3c * x * z; dY[10][2] = kSH3c * x * y;
+    Y[11] = y * (kSH3d - kSH3e * zz); dY[11][0] = 0; dY[11][1] = kSH3d - kSH3e * zz; dY[11][2] = -2.0f * kSH3e * y * z;
+    Y[12] = z * (kSH3f * zz - kSH3g); dY[12][0] = 0; dY[12][1] = 0; dY[12][2] = 3.0f * kSH3f * zz - kSH3g;
+    Y[13] = x * (kSH3d - kSH3e * zz); dY[13][0] = kSH3d - kSH3e * zz; dY[13][1] = 0; dY[13][2] = -2.0f * kSH3e * x * z;
+    Y[14] = kSH3h * z * (xx - yy); dY[14][0] = 2.0f * kSH3h * x * z; dY[14][1] = -2.0f * kSH3h * y * z; dY[14][2] = kSH3h * (xx - yy);
+    Y[15] = x * (kSH3b * yy - kSH3a * xx); dY[15][0] = kSH3b * yy - 3.0f * kSH3a * xx; dY[15][1] = 2.0f * kSH3b * x * y; dY[15][2] = 0;
+}
+
+// Projection backward (gs_utils.h:38-193 differentiated): accumulated projected-quantity gradients to
+// the parameters. Culled Gaussians receive zero gradients.
+__global__ void __launch_bounds__(kBlock) projection_backward_kernel(const BackwardParams b) {
+    const uint32_t g = blockIdx.x * kBlock + threadIdx.x;
+    if (g >= b.n) return;
+    const float* acc = b.accum + static_cast<size_t>(g) * kAccum;
+    float* dm = b.d_means + 3 * g;
+    float* ds = b.d_scales + 3 * g;
+    float* dq = b.d_rotations + 4 * g;
+    float* dsh = b.d_sh + static_cast<size_t>(g) * b.sh_bases * 3;
+    dm[0] = dm[1] = dm[2] = 0.0f;
+    ds[0] = ds[1] = ds[2] = 0.0f;
+    dq[0] = dq[1] = dq[2] = dq[3] = 0.0f;
+    b.d_opacities[g] = 0.0f;
+    for (uint32_t i = 0; i < b.sh_bases * 3; ++i) dsh[i] = 0.0f;
+    bool any = false;
+    for (int i = 0; i < kAccum; ++i) any |= acc[i] != 0.0f;
+    if (!any) return;
+
+    const float mx = b.means[3 * g], my = b.means[3 * g + 1], mz = b.means[3 * g + 2];
+    const float4 r1 = b.w2c[0], r2 = b.w2c[1], r3 = b.w2c[2];
+    const float tx = r1.x * mx + r1.y * my + r1.z * mz + r1.w;
+    const float ty = r2.x * mx + r2.y * my + r2.z * mz + r2.w;
+    const float tz = r3.x * mx + r3.y * my + r3.z * mz + r3.w;
+    const float x = tx / tz, y = ty / tz;
+    const PassCamera& cam = b.cam;
+    const float cl = (-0.15f * cam.width - cam.center_x) / cam.focal_x, cr = (1.15f * cam.width - cam.center_x) / cam.focal_x;
+    const float ct = (-0.15f * cam.height - cam.center_y) / cam.focal_y, cb = (1.15f * cam.height - cam.center_y) / cam.focal_y;
+    const float xc = fminf(fmaxf(x, cl), cr), yc = fminf(fmaxf(y, ct), cb);
+    const bool free_x = x > cl && x < cr, free_y = y > ct && y < cb;
+    // rotation of the normalised quaternion
+    const float4 q = b.rotations[g];
+    const float qnorm = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    const float w = q.x / qnorm, X = q.y / qnorm, Yq = q.z / qnorm, Z = q.w / qnorm;
+    const float R[3][3] = {{1 - 2 * (Yq * Yq + Z * Z), 2 * (X * Yq - w * Z), 2 * (X * Z + w * Yq)},
+                           {2 * (X * Yq + w * Z), 1 - 2 * (X * X + Z * Z), 2 * (Yq * Z - w * X)},
+                           {2 * (X * Z - w * Yq), 2 * (Yq * Z + w * X), 1 - 2 * (X * X + Yq * Yq)}};
+    const float v[3] = {expf(2.0f * b.scales[3 * g]), expf(2.0f * b.scales[3 * g + 1]), expf(2.0f * b.scales[3 * g + 2])};
+    float S[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) S[i][j] = R[i][0] * v[0] * R[j][0] + R[i][1] * v[1] * R[j][1] + R[i][2] * v[2] * R[j][2];
+    const float W3[3][3] = {{r1.x, r1.y, r1.z}, {r2.x, r2.y, r2.z}, {r3.x, r3.y, r3.z}};
+    const float J[2][3] = {{cam.focal_x / tz, 0.0f, -cam.focal_x * xc / tz}, {0.0f, cam.focal_y / tz, -cam.focal_y * yc / tz}};
+    float T[2][3];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 3; ++j) T[i][j] = J[i][0] * W3[0][j] + J[i][1] * W3[1][j] + J[i][2] * W3[2][j];
+    float cov[2][2];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) {
+            float s = 0.0f;
+            for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l) s += T[i][k] * S[k][l] * T[j][l];
+            cov[i][j] = s;
+        }
+    const float dil = kDilation * cam.ss * cam.ss;
+    const float a = cov[0][0] + dil, bb = cov[0][1], c = cov[1][1] + dil;
+    const float det = a * c - bb * bb;
+    const float C[2][2] = {{c / det, -bb / det}, {-bb / det, a / det}};
+    const float op = 1.0f / (1.0f + expf(-b.opacities[g]));
+
+    // opacity logit
+    b.d_opacities[g] = acc[0] * op * (1.0f - op);
+    // conic = inverse(cov2d + dilation)
+    const float G[2][2] = {{acc[1], 0.5f * acc[2]}, {0.5f * acc[2], acc[3]}};
+    float CG[2][2], GA[2][2];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) CG[i][j] = C[i][0] * G[0][j] + C[i][1] * G[1][j];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) GA[i][j] = -(CG[i][0] * C[0][j] + CG[i][1] * C[1][j]);
+    float dS[3][3], dT[2][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float s = 0.0f;
+            for (int k = 0; k < 2; ++k)
+                for (int l = 0; l < 2; ++l) s += T[k][i] * GA[k][l] * T[l][j];
+            dS[i][j] = s;
+        }
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float s = 0.0f;
+            for (int k = 0; k < 2; ++k)
+                for (int l = 0; l < 3; ++l) s += GA[i][k] * T[k][l] * S[l][j];
+            dT[i][j] = 2.0f * s;
+        }
+    float dJ[2][3];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 3; ++j) dJ[i][j] = dT[i][0] * W3[j][0] + dT[i][1] * W3[j][1] + dT[i][2] * W3[j][2];
+    float dtz = acc[6];
+    dtz += dJ[0][0] * (-cam.focal_x / (tz * tz)) + dJ[0][2] * (cam.focal_x * xc / (tz * tz)) +
+           dJ[1][1] * (-cam.focal_y / (tz * tz)) + dJ[1][2] * (cam.focal_y * yc / (tz * tz));
+    float dxv = acc[4] * cam.focal_x, dyv = acc[5] * cam.focal_y;
+    if (free_x) dxv += dJ[0][2] * (-cam.focal_x / tz);
+    if (free_y) dyv += dJ[1][2] * (-cam.focal_y / tz);
+    const float dtx = dxv / tz, dty = dyv / tz;
+    dtz -= dxv * tx / (tz * tz) + dyv * ty / (tz * tz);
+    float gm[3];
+    for (int i = 0; i < 3; ++i) gm[i] = W3[0][i] * dtx + W3[1][i] * dty + W3[2][i] * dtz;
+    // covariance = R V R^T
+    for (int i = 0; i < 3; ++i) {
+        float s = 0.0f;
+        for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) s += R[k][i] * dS[k][l] * R[l][i];
+        ds[i] = s * 2.0f * v[i];
+    }
+    float dR[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float s = 0.0f;
+            for (int k = 0; k < 3; ++k) s += (dS[i][k] + dS[k][i]) * R[k][j];
+            dR[i][j] = s * v[j];
+        }
+    float dqn[4];
+    dqn[0] = 2 * (-Z * dR[0][1] + Yq * dR[0][2] + Z * dR[1][0] - X * dR[1][2] - Yq * dR[2][0] + X * dR[2][1]);
+    dqn[1] = 2 * (Yq * dR[0][1] + Z * dR[0][2] + Yq * dR[1][0] - 2 * X * dR[1][1] - w * dR[1][2] + Z * dR[2][0] +
+                  w * dR[2][1] - 2 * X * dR[2][2]);
+    dqn[2] = 2 * (-2 * Yq * dR[0][0] + X * dR[0][1] + w * dR[0][2] + X * dR[1][0] + Z * dR[1][2] - w * dR[2][0] +
+                  Z * dR[2][1] - 2 * Yq * dR[2][2]);
+    dqn[3] = 2 * (-2 * Z * dR[0][0] - w * dR[0][1] + X * dR[0][2] + w * dR[1][0] - 2 * Z * dR[1][1] + Yq * dR[1][2] +
+                  X * dR[2][0] + Yq * dR[2][1]);
+    const float dot = dqn[0] * w + dqn[1] * X + dqn[2] * Yq + dqn[3] * Z;
+    dq[0] = (dqn[0] - w * dot) / qnorm;
+    dq[1] = (dqn[1] - X * dot) / qnorm;
+    dq[2] = (dqn[2] - Yq * dot) / qnorm;
+    dq[3] = (dqn[3] - Z * dot) / qnorm;
+    // colour = max(0.5 + sum Y_b sh_b, 0); direction = normalize(mean - camera)
+    const float dvx = mx - b.cam_position[0], dvy = my - b.cam_position[1], dvz = mz - b.cam_position[2];
+    const float len = sqrtf(dvx * dvx + dvy * dvy + dvz * dvz);
+    const float dir[3] = {dvx / len, dvy / len, dvz / len};
+    float Y[16], dY[16][3];
+    sh_basis(dir[0], dir[1], dir[2], Y, dY);
+    const float* shg = b.sh + static_cast<size_t>(g) * b.sh_bases * 3;
+    const float* col = b.colors + 3 * g;
+    float ddir[3] = {0.0f, 0.0f, 0.0f};
+    for (int ch = 0; ch < 3; ++ch) {
+        const float gc = col[ch] > 0.0f ? acc[7 + ch] : 0.0f;
+        for (uint32_t k = 0; k < b.sh_bases; ++k) {
+            dsh[3 * k + ch] = gc * Y[k];
+            ddir[0] += gc * shg[3 * k + ch] * dY[k][0];
+            ddir[1] += gc * shg[3 * k + ch] * dY[k][1];
+            ddir[2] += gc * shg[3 * k + ch] * dY[k][2];
+        }
+    }
+    const float dd = ddir[0] * dir[0] + ddir[1] * dir[1] + ddir[2] * dir[2];
+    for (int k = 0; k < 3; ++k) dm[k] = gm[k] + (ddir[k] - dir[k] * dd) / len;
+}
+
+}  // namespace
+
+cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream) {
+    if (p.n == 0) return cudaSuccess;
+    colors_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_fragments(const BackwardParams& p, cudaStream_t stream) {
+    if (p.n == 0) return cudaSuccess;
+    fragments_backward_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_projection(const BackwardParams& p, cudaStream_t stream) {
+    if (p.n == 0) return cudaSuccess;
+    projection_backward_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace sgs

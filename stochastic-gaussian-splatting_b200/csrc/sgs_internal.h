@@ -120,6 +120,39 @@ struct ResolveParams {
 
 cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream);
 
+// Backward pass of stochastic transparency (backward_st.cu).
+struct BackwardParams {
+    const float* means;
+    const float* scales;
+    const float4* rotations;
+    const float* opacities;
+    const float* sh;
+    const float4* w2c;
+    const float* cam_position;
+    uint32_t n;
+    uint32_t sh_bases;
+    PassCamera cam;                          // framebuffer camera
+    uint32_t width;                          // image width (pixels)
+    uint32_t ss;
+    const unsigned long long* framebuffer;   // the sample's winners
+    const float4* samples;                   // the sample's winner colour and depth
+    const float* grad_image;                 // (H, W, 3) upstream gradient of the image
+    const float* grad_alpha;                 // (H, W) or null
+    const float* grad_depth;                 // (H, W) or null
+    float grad_scale;                        // weight of this sample in the output / ss^2
+    float* colors;                           // (N, 3) per-Gaussian colour
+    float* accum;                            // (N, 10) projected-quantity gradients
+    float* d_means;
+    float* d_scales;
+    float* d_rotations;
+    float* d_opacities;
+    float* d_sh;
+};
+
+cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream);
+cudaError_t launch_backward_fragments(const BackwardParams& p, cudaStream_t stream);
+cudaError_t launch_backward_projection(const BackwardParams& p, cudaStream_t stream);
+
 // Sets the calling thread's sgs_last_error() message (printf format) and returns `status`.
 int record_error(int status, const char* fmt, ...);
 
