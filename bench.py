@@ -342,9 +342,46 @@ def run_ours(args, world, rank, local) -> dict | None:
     }
     if not args.no_batch and args.workload.startswith("batch_6m"):
         line["batch32_graph"] = batch_graph(scene, fl, dev, steps=max(4, args.steps // 8))
+    if not args.no_train and args.workload.startswith("batch_6m"):
+        del scene
+        torch.cuda.empty_cache()
+        line["train_step"] = train_measure(dev)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_cpu, cam, fl, args.cpu_frames, args.workload)
     return line
+
+
+def train_measure(dev, views: int = 4, target_spp: int = 64, steps_per_view: int = 2) -> dict:
+    """Differentiable training step of the 500k-Gaussian 800x800 workload: 8 samples forward, L1 +
+    0.2 (1 - SSIM), hand-written backward to all parameters, Adam update (targets at 64 spp here)."""
+    import sgs_train
+
+    scene, cams, targets = sgs_train.make_problem(views=views, target_spp=target_spp, device=dev)
+    params = [t.to(dev).requires_grad_(True) for t in scene.tensors()]
+    opt = torch.optim.Adam(params, lr=1e-3)
+    settings = [sgs_train.view_settings(c, dev) for c in cams]
+    losses = []
+    # warm-up (allocations, autotuning of torch's conv) then timed steps
+    for i in range(views):
+        opt.zero_grad(set_to_none=True)
+        losses.append(float(sgs_train.train_step(params, settings[i], targets[i])))
+        opt.step()
+    torch.cuda.synchronize(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = views * steps_per_view
+    t0.record()
+    last = []
+    for k in range(n):
+        opt.zero_grad(set_to_none=True)
+        last.append(sgs_train.train_step(params, settings[k % views], targets[k % views]))
+        opt.step()
+    t1.record()
+    torch.cuda.synchronize(dev)
+    ms = t0.elapsed_time(t1) / n
+    return {"gaussians": int(scene.means.shape[0]), "resolution": "800x800", "spp_per_step": 8,
+            "ms_per_step": round(ms, 3), "steps_per_s": round(1000.0 / ms, 2),
+            "loss_first_epoch": round(sum(losses) / len(losses), 5),
+            "loss_last_epoch": round(float(sum(last[-views:]) / views), 5)}
 
 
 def batch_graph(scene, fl, dev, steps: int) -> dict:
@@ -460,6 +497,7 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 32-view CUDA-graph measurement")
+    ap.add_argument("--no-train", action="store_true", help="skip the differentiable training-step measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         # reference semantics on the host cores; no GPU work, no process group needed
