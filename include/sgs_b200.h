@@ -158,6 +158,79 @@ int sgs_backward_finish(const sgs_gaussians* gaussians, const sgs_camera* camera
                         void* backward_workspace, float* d_means, float* d_scales, float* d_rotations,
                         float* d_opacities, float* d_sh, void* stream);
 
+/* ---- Learned resolve (no counterpart in the reference) ------------------------------------------
+ * A 6-layer 3x3 convolutional denoiser (8 -> 32 -> 32 -> 32 -> 32 -> 32 -> 3, ReLU between layers,
+ * the last layer adds the mean colour back) that maps a few samples' features to the converged
+ * image; plain progressive averaging (SGS_TEMPORAL_STATIC) stays the fallback. BF16 operands on the
+ * sm_100a tensor cores (tcgen05), FP32 accumulation.
+ *
+ * Image arrays are NHWC: [batch][height][width][channels], 16-byte aligned. Features are FP16 with
+ * 8 channels (sgs_denoise_features_finalize); activations and their gradients are BF16 with 16 or
+ * 32 channels; the output is FP32 RGB [batch][height][width][3], premultiplied like `History`.
+ *
+ * Packed weights of one layer, BF16, [tap = 3 dy + dx][in_channel / 8][out_channel][in_channel % 8]
+ * (features count as 16 input channels, 8..15 zero). A forward layer with weights W[co][ci][dy][dx]
+ * (cross-correlation, zero padding 1) packs W; its data gradient packs W'[tap][n = ci][k = co] =
+ * W[8 - tap][co][ci] and runs with the mask epilogue. */
+#define SGS_DENOISE_LAYERS 6
+#define SGS_DENOISE_WIDTH 32   /* hidden channels */
+#define SGS_DENOISE_FEATURES 8 /* FP16 input channels: mean rgb, mean alpha, mean depth x scale,
+                                  standard error of the mean luminance, winner change rate, 0 */
+
+enum sgs_conv_epilogue {
+    SGS_CONV_RELU = 0,  /* out = relu(conv + bias), BF16 */
+    SGS_CONV_FINAL = 1, /* out[0..2] = conv[0..2] + bias[0..2] + residual features[0..2], FP32 RGB */
+    SGS_CONV_MASK = 2   /* out = conv * (mask > 0), BF16: the data gradient through the ReLU below */
+};
+
+typedef struct sgs_conv3x3_args {
+    const void* input;    /* in_channels 8: FP16 features; 16 or 32: BF16 */
+    void* output;
+    const void* weights;  /* sgs_conv3x3_weights_size(in, out) bytes, packed as above */
+    const float* bias;    /* (out_channels); unused by SGS_CONV_MASK */
+    const void* mask;     /* SGS_CONV_MASK: BF16 [..][out_channels] activation of the layer below */
+    const void* residual; /* SGS_CONV_FINAL: the FP16 features */
+    int32_t batch, height, width;
+    int32_t in_channels;  /* 8 (features), 16 or 32 */
+    int32_t out_channels; /* 16 or 32 */
+    int32_t epilogue;     /* sgs_conv_epilogue */
+} sgs_conv3x3_args;
+
+/* Supported (in, out, epilogue): (8, 32, RELU), (32, 32, RELU), (32, 16, FINAL), (32, 32, MASK),
+ * (16, 32, MASK). */
+size_t sgs_conv3x3_weights_size(int32_t in_channels, int32_t out_channels);
+int sgs_conv3x3(const sgs_conv3x3_args* conv, void* stream);
+
+/* Adds the weight gradient sum_p dZ[p][co] * X[p + tap][ci] to grad_weights, FP32
+ * [9][out_channels][16 or 32] (features count as 16 input channels), and sum_p dZ[p][co] to
+ * grad_bias (out_channels). X is the layer input (as in sgs_conv3x3), dZ the BF16 gradient of the
+ * layer output before its activation, [..][out_channels]. Supported (in, out): (8, 32), (32, 32),
+ * (32, 16). Summation order is not fixed (atomic adds). */
+int sgs_conv3x3_wgrad(const void* input, int32_t in_channels, const void* grad_output, int32_t out_channels,
+                      int32_t batch, int32_t height, int32_t width, float* grad_weights, float* grad_bias,
+                      void* stream);
+
+/* Features of a run of samples. For every sample (a Reset-mode render: its image, alpha and depth,
+ * and optionally the winner framebuffer of the render workspace, (depth bits << 32 | index) per
+ * pixel at supersampling 1), accumulate into `accum` (8 floats per pixel; `first` starts the sums);
+ * then finalize into the FP16 features. */
+int sgs_denoise_features_accumulate(const float* image, const float* alpha, const float* depth,
+                                    const uint64_t* framebuffer, float* accum, uint32_t n_pixels, int32_t first,
+                                    void* stream);
+int sgs_denoise_features_finalize(const float* accum, uint32_t n_pixels, uint32_t n_samples, float depth_scale,
+                                  void* features, void* stream);
+
+/* The whole denoiser: features -> FP32 RGB. `weights` holds the 6 packed layers back to back
+ * (sgs_denoise_weights_size() bytes), `biases` 32 x 5 + 16 floats (the last layer's 3 used). */
+size_t sgs_denoise_weights_size(void);
+size_t sgs_denoise_scratch_size(int32_t batch, int32_t height, int32_t width);
+int sgs_denoise(const void* features, int32_t batch, int32_t height, int32_t width, const void* weights,
+                const float* biases, void* scratch, size_t scratch_bytes, float* output, void* stream);
+
+/* Synchronises `stream` and reports whether a denoiser kernel gave up a bounded tensor-core wait
+ * (SGS_ERROR_CUDA), clearing the flag. */
+int sgs_denoise_status(void* stream);
+
 /* Diagnostics (no counterpart in the reference): CUDA events (cudaEvent_t) that the calling
  * thread's next sgs_render calls record on their stream immediately before the first and after the
  * last kernel of the accumulate stage, so that callers can time that stage with cudaEventElapsedTime.

@@ -90,6 +90,27 @@ class WorkspaceLayout(ctypes.Structure):
     ]
 
 
+class Conv3x3Args(ctypes.Structure):
+    _fields_ = [
+        ("input", ctypes.c_void_p),
+        ("output", ctypes.c_void_p),
+        ("weights", ctypes.c_void_p),
+        ("bias", ctypes.c_void_p),
+        ("mask", ctypes.c_void_p),
+        ("residual", ctypes.c_void_p),
+        ("batch", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("in_channels", ctypes.c_int32),
+        ("out_channels", ctypes.c_int32),
+        ("epilogue", ctypes.c_int32),
+    ]
+
+
+SGS_CONV_RELU = 0
+SGS_CONV_FINAL = 1
+SGS_CONV_MASK = 2
+
 # every entry point of include/sgs_b200.h: name -> (restype, argtypes)
 SIGNATURES = {
     "sgs_workspace_size": (ctypes.c_size_t, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC)]),
@@ -110,6 +131,22 @@ SIGNATURES = {
                                            ctypes.POINTER(SettingsC), ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "sgs_conv3x3_weights_size": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    "sgs_conv3x3": (ctypes.c_int, [ctypes.POINTER(Conv3x3Args), ctypes.c_void_p]),
+    "sgs_conv3x3_wgrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_denoise_features_accumulate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                       ctypes.c_int32, ctypes.c_void_p]),
+    "sgs_denoise_features_finalize": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                                     ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_denoise_weights_size": (ctypes.c_size_t, []),
+    "sgs_denoise_scratch_size": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "sgs_denoise": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                   ctypes.c_void_p]),
+    "sgs_denoise_status": (ctypes.c_int, [ctypes.c_void_p]),
     "sgs_set_stage_events": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_get_frame_index": (ctypes.c_uint32, []),
     "sgs_set_frame_index": (None, [ctypes.c_uint32]),

@@ -32,6 +32,7 @@ def test_struct_layout_matches_the_header(tmp_path):
     structs = {
         "sgs_gaussians": _abi.Gaussians, "sgs_camera": _abi.Camera, "sgs_settings": _abi.SettingsC,
         "sgs_history": _abi.HistoryC, "sgs_outputs": _abi.Outputs, "sgs_workspace_layout": _abi.WorkspaceLayout,
+        "sgs_conv3x3_args": _abi.Conv3x3Args,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void) {']
     for cname, cls in structs.items():
