@@ -219,14 +219,15 @@ class FeatureAccumulator:
         self.n = 0
 
     def add(self, image: torch.Tensor, alpha: torch.Tensor, depth: torch.Tensor,
-            framebuffer: torch.Tensor | None = None) -> None:
+            framebuffer: torch.Tensor | None = None, first: bool | None = None) -> None:
         dev = self.accum.device
+        first = self.n == 0 if first is None else first
         _check(_lib.sgs_denoise_features_accumulate(
             ctypes.c_void_p(image.data_ptr()), ctypes.c_void_p(alpha.data_ptr()), ctypes.c_void_p(depth.data_ptr()),
             None if framebuffer is None else ctypes.c_void_p(framebuffer.data_ptr()),
-            ctypes.c_void_p(self.accum.data_ptr()), self.n_px, int(self.n == 0), _stream(dev)),
+            ctypes.c_void_p(self.accum.data_ptr()), self.n_px, int(first), _stream(dev)),
             "sgs_denoise_features_accumulate")
-        self.n += 1
+        self.n = 1 if first else self.n + 1
 
     def finalize(self, depth_scale: float, out: torch.Tensor | None = None) -> torch.Tensor:
         if out is None:
@@ -263,3 +264,85 @@ def render_features(tensors, settings: Settings, n_samples: int, first_frame: in
     if checkpoints:
         return marks
     return acc.finalize(depth_scale)
+
+
+class CapturedFeatures:
+    """`render_features` with each sample after the first replayed from a CUDA graph.
+
+    One graph holds a Reset-mode render (frame index from a device counter, advanced on the GPU)
+    and its feature accumulation, so the host issues one replay per sample. The scene tensors, the
+    camera pose (`w2c`, `position`) and the accumulator are captured by address: `set_scene` and
+    `set_pose` copy new values into them; the resolution and intrinsics stay those of `settings`.
+    Frames first_frame .. first_frame + n - 1 give the same features as `render_features`.
+    """
+
+    def __init__(self, tensors, settings: Settings, depth_scale: float):
+        self.device = tensors[0].device
+        self.tensors = tuple(t.clone() for t in tensors)
+        self.settings = settings._replace(w2c=settings.w2c.clone().contiguous(),
+                                          cam_position=settings.cam_position.clone().contiguous())
+        self.depth_scale = depth_scale
+        h, w = settings.height, settings.width
+        self.ss = max(1, settings.supersampling_factor)
+        self.n_fb = w * h * self.ss ** 2
+        self.acc = FeatureAccumulator(h, w, self.device)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.kb = (torch.empty((0, self.n_fb, 2), dtype=torch.int32, device=self.device),
+                   torch.empty((0, self.n_fb, 4), device=self.device))
+        self.eye = torch.eye(4, device=self.device)
+        self.blue = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self.graph = None
+
+    def _step(self, first: bool):
+        e = torch.empty(0)
+        outs, ws, layout = _C.render_with_workspace(*self.tensors, *self.settings.as_tuple(), self.blue, *self.kb,
+                                                    e, e, e, e, self.eye, 0)
+        fb = _C.workspace_views(ws, layout, self.n_fb, False)["framebuffer"] if self.ss == 1 else None
+        self.acc.add(outs[0], outs[2], outs[1], fb, first=first)
+        return outs, ws
+
+    def capture(self) -> "CapturedFeatures":
+        _C.set_device_frame_counter(self.counter)
+        try:
+            stream = torch.cuda.Stream(self.device)
+            stream.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(stream):
+                self._step(first=True)
+            torch.cuda.current_stream(self.device).wait_stream(stream)
+            torch.cuda.synchronize(self.device)
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._kept = self._step(first=False)
+        finally:
+            _C.set_device_frame_counter(None, self.device)
+        return self
+
+    def set_scene(self, tensors) -> None:
+        for d, s in zip(self.tensors, tensors):
+            d.copy_(s)
+
+    def set_pose(self, w2c: torch.Tensor, position: torch.Tensor) -> None:
+        self.settings.w2c.copy_(w2c)
+        self.settings.cam_position.copy_(position)
+
+    def run(self, n_samples: int, first_frame: int, checkpoints=()):
+        """Features of n_samples samples (FP16 [H, W, 8]), or {count: features} at `checkpoints`."""
+        if self.graph is None:
+            self.capture()
+        self.counter.fill_(first_frame)
+        _C.set_device_frame_counter(self.counter)
+        try:
+            self._step(first=True)
+        finally:
+            _C.set_device_frame_counter(None, self.device)
+        marks = {}
+        if 1 in checkpoints:
+            marks[1] = self.acc.finalize(self.depth_scale)
+        for s in range(1, n_samples):
+            self.graph.replay()
+            self.acc.n = s + 1
+            if s + 1 in checkpoints:
+                marks[s + 1] = self.acc.finalize(self.depth_scale)
+        if checkpoints:
+            return marks
+        return self.acc.finalize(self.depth_scale)

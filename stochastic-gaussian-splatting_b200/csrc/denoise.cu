@@ -439,13 +439,26 @@ int sm_count() {
     return count;
 }
 
+// CTAs of `kernel` that fit on one SM, from its shared memory (with the maximum carveout), registers
+// and threads; at most `cap`. (The occupancy query answers for the default carveout, which keeps
+// these small-footprint kernels at one CTA per SM.)
 template <typename Kernel>
 int resident_ctas(Kernel kernel, size_t smem, int cap) {
-    int blocks = 0;
+    int dev = 0, smem_sm = 0, regs_sm = 0;
+    cudaFuncAttributes attr{};
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
             cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kThreads, smem) != cudaSuccess)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+            cudaSuccess ||
+        cudaFuncGetAttributes(&attr, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess)
         return 0;
+    const size_t per_cta = smem + attr.sharedSizeBytes + 1024;  // 1 KB reserved per CTA
+    int blocks = static_cast<int>(static_cast<size_t>(smem_sm) / per_cta);
+    const int regs = attr.numRegs > 0 ? attr.numRegs * kThreads : 1;
+    if (regs_sm / regs < blocks) blocks = regs_sm / regs;
+    if (2048 / kThreads < blocks) blocks = 2048 / kThreads;
     return blocks < cap ? blocks : cap;
 }
 

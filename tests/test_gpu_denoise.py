@@ -192,3 +192,21 @@ def test_features_match_torch(cuda_device):
     assert feats.shape == (47, 61, 8)
     assert (feats - ref).abs().max() < 2e-3 * max(1.0, float(ref.abs().max())), float((feats - ref).abs().max())
     assert change.max() > 0  # the scene is noisy enough that winners change
+
+
+def test_captured_features_equal_eager(cuda_device):
+    scene = sgs_scenes.make_scene(sgs_scenes.SceneSpec(n=4000, log_scale_mean=-3.0), seed=8)
+    cams = [sgs_scenes.pinhole((0.5, 0.2, -4.0), 64, 40, 60.0), sgs_scenes.pinhole((-1.0, 0.0, -3.5), 64, 40, 60.0)]
+    tensors = tuple(t.cuda() for t in scene.tensors())
+
+    def settings(cam):
+        return Settings(cam.w2c.cuda(), cam.position.cuda(), cam.width, cam.height, cam.focal_x, cam.focal_y,
+                        cam.center_x, cam.center_y, cam.near_plane, cam.far_plane, False, 1, False, False, False)
+
+    sampler = dn.CapturedFeatures(tensors, settings(cams[0]), 0.5).capture()
+    for i, cam in enumerate(cams):
+        sampler.set_pose(cam.w2c.cuda(), cam.position.cuda())
+        got = sampler.run(9, first_frame=50 + 100 * i, checkpoints=(1, 4, 9))
+        want = dn.render_features(tensors, settings(cam), 9, 50 + 100 * i, 0.5, checkpoints=(1, 4, 9))
+        for k in (1, 4, 9):
+            assert torch.equal(got[k], want[k]), (i, k)
