@@ -48,8 +48,21 @@ DEFAULT_WORKLOAD = "batch_6m_1080_st"
 # `ncu --set full` (profiles/st_scatter_kernel_batch_6m_1080.md)
 NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 278.58e6 + 15.51e6}
 
-# measured copy bandwidth of this pool's B200s when MEASURED_PEAKS.json is absent
+# measured copy bandwidth and bf16 GEMM rate of this pool's B200s when MEASURED_PEAKS.json is absent
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
+
+DENOISER_WEIGHTS = ROOT / "stochastic-gaussian-splatting_b200" / "StochasticGSCudaBackend" / "denoiser_c2.npz"
+
+
+def bf16_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        try:
+            return float(json.loads(path.read_text())["bf16_tflops"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return FALLBACK_BF16_TFLOPS, "fallback"
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -342,13 +355,59 @@ def run_ours(args, world, rank, local) -> dict | None:
     }
     if not args.no_batch and args.workload.startswith("batch_6m"):
         line["batch32_graph"] = batch_graph(scene, fl, dev, steps=max(4, args.steps // 8))
-    if not args.no_train and args.workload.startswith("batch_6m"):
+    if not (args.no_train and args.no_learned) and args.workload.startswith("batch_6m"):
         del scene
         torch.cuda.empty_cache()
+    if not args.no_learned and args.workload == "batch_6m_1080_st":
+        line["learned_resolve"] = learned_resolve_measure(dev)
+        torch.cuda.empty_cache()
+    if not args.no_train and args.workload.startswith("batch_6m"):
         line["train_step"] = train_measure(dev)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_cpu, cam, fl, args.cpu_frames, args.workload)
     return line
+
+
+def learned_resolve_measure(dev) -> dict:
+    """The learned resolve on the 6M scene at 1920x1080 with the committed weights: one sgs_denoise
+    call timed with CUDA events (six tensor-core conv launches) against the bf16 tensor peak and
+    HBM; PSNR / SSIM of learned and plain resolves at 4, 16, 64 and 256 samples against a
+    4096-sample ground truth (one orbit view); the equal-PSNR time against 256 plain samples."""
+    import numpy as np
+
+    import sgs_denoise_train
+    from StochasticGSCudaBackend import denoise as dn
+
+    trained = DENOISER_WEIGHTS.is_file()
+    model = dn.Denoiser.from_state(np.load(DENOISER_WEIGHTS), device=dev) if trained else dn.Denoiser(device=dev)
+    rep = sgs_denoise_train.evaluate(model, views=1, log=None, device=dev)
+    px = 1920 * 1080
+    flops = 2 * 9 * sum(ci * co for ci, co in dn.LAYERS) * px
+    # per pixel: features read twice (layer 1, residual) 32 B, five activations written and read
+    # back 5 x 128 B, RGB out 12 B
+    hbm_bytes = (32 + 5 * 128 + 12) * px
+    ms = rep["denoise_ms"]
+    peak, src = bf16_peak()
+    hpeak, _ = hbm_peak()
+    tflops = flops / (ms * 1e-3) / 1e12
+    gbs = hbm_bytes / (ms * 1e-3) / 1e9
+    return {
+        "weights": "trained (denoiser_c2.npz)" if trained else "untrained (plain average)",
+        "denoise_ms_1080p": round(ms, 4),
+        "roofline": {"bound": "hbm", "kernels": "conv3x3_tma_kernel x5 + conv3x3_kernel (layer 1)",
+                     "achieved": round(gbs, 1), "peak": hpeak, "unit": "GB/s", "frac": round(gbs / hpeak, 4),
+                     "algorithmic_bytes_per_call": hbm_bytes,
+                     "tensor": {"achieved_tflops": round(tflops, 1), "peak_tflops": peak, "peak_source": src,
+                                "frac": round(tflops / peak, 4), "flops_per_call": flops}},
+        "psnr_db": {k: {"plain": round(v["plain_psnr"], 3), "learned": round(v["learned_psnr"], 3)}
+                    for k, v in rep["table"].items()},
+        "ssim": {k: {"plain": round(v["plain_ssim"], 4), "learned": round(v["learned_ssim"], 4)}
+                 for k, v in rep["table"].items()},
+        "plain_ms_per_sample": round(rep["plain_ms_per_sample"], 4),
+        "feature_ms_per_sample": round(rep["feature_ms_per_sample"], 4),
+        "equal_psnr": rep["equal_psnr"],
+        "ground_truth_spp": rep["gt_spp"],
+    }
 
 
 def train_measure(dev, views: int = 4, target_spp: int = 64, steps_per_view: int = 2) -> dict:
@@ -498,6 +557,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 32-view CUDA-graph measurement")
     ap.add_argument("--no-train", action="store_true", help="skip the differentiable training-step measurement")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-resolve measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         # reference semantics on the host cores; no GPU work, no process group needed

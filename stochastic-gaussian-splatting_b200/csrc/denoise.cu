@@ -31,6 +31,8 @@
 // sgs_denoise_status), stops, waits once more with a bound, releases its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -143,8 +145,49 @@ __device__ __forceinline__ void load_accumulator(uint32_t taddr, float (&acc)[N]
     tc::tmem_wait_ld();
 }
 
+// Epilogue of one output pixel (thread m of the tile owns pixel m = 8 * row + column): bias and
+// ReLU, bias and residual (final layer), or the ReLU mask of the layer below (data gradient).
+template <int COUT, int EPI>
+__device__ __forceinline__ void store_pixel(const ConvArgs& a, const TileXY& tile, int m, const float (&acc)[COUT],
+                                            const float (&bias)[COUT]) {
+    const int x = tile.x0 + (m & 7), y = tile.y0 + (m >> 3);
+    if (x >= a.width || y >= a.height) return;
+    const size_t pixel = (static_cast<size_t>(tile.b) * a.height + y) * a.width + x;
+    if constexpr (EPI == kEpiFinal) {
+        const uint4 r = __ldg(a.residual + pixel);
+        const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
+        const float2 bx = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
+        float* out = static_cast<float*>(a.out) + pixel * 3;
+        out[0] = acc[0] + bias[0] + rg.x;
+        out[1] = acc[1] + bias[1] + rg.y;
+        out[2] = acc[2] + bias[2] + bx.x;
+    } else {
+        uint4* out = static_cast<uint4*>(a.out) + pixel * (COUT / 8);
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q) {
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = acc[8 * q + i] + bias[8 * q + i];
+            if constexpr (EPI == kEpiRelu) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = fmaxf(v[i], 0.0f);
+            } else {
+                const uint4 mk = __ldg(a.mask + pixel * (COUT / 8) + q);
+                const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (!(bf16_lo(mw[i]) > 0.0f)) v[2 * i] = 0.0f;
+                    if (!(bf16_hi(mw[i]) > 0.0f)) v[2 * i + 1] = 0.0f;
+                }
+            }
+            out[q] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                                pack_bf16(v[6], v[7]));
+        }
+    }
+}
+
 template <int CIN, int COUT, int IN, int EPI>
-__global__ void __launch_bounds__(kThreads) conv3x3_kernel(const ConvArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) conv3x3_kernel(const ConvArgs a) {
     constexpr int KC = CIN / 8;
     constexpr int kWeightVecs = 9 * KC * COUT;
     constexpr int kHaloVecs = KC * kHaloPx;
@@ -203,41 +246,7 @@ __global__ void __launch_bounds__(kThreads) conv3x3_kernel(const ConvArgs a) {
         float acc[COUT];
         load_accumulator<COUT>(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
 
-        const int x = tile.x0 + (tid & 7), y = tile.y0 + (tid >> 3);
-        if (ok && x < a.width && y < a.height) {
-            const size_t pixel = (static_cast<size_t>(tile.b) * a.height + y) * a.width + x;
-            if constexpr (EPI == kEpiFinal) {
-                const uint4 r = __ldg(a.residual + pixel);
-                const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
-                const float2 bx = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
-                float* out = static_cast<float*>(a.out) + pixel * 3;
-                out[0] = acc[0] + bias[0] + rg.x;
-                out[1] = acc[1] + bias[1] + rg.y;
-                out[2] = acc[2] + bias[2] + bx.x;
-            } else {
-                uint4* out = static_cast<uint4*>(a.out) + pixel * (COUT / 8);
-#pragma unroll
-                for (int q = 0; q < COUT / 8; ++q) {
-                    float v[8];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) v[i] = acc[8 * q + i] + bias[8 * q + i];
-                    if constexpr (EPI == kEpiRelu) {
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) v[i] = fmaxf(v[i], 0.0f);
-                    } else {
-                        const uint4 m = __ldg(a.mask + pixel * (COUT / 8) + q);
-                        const uint32_t mw[4] = {m.x, m.y, m.z, m.w};
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            if (!(bf16_lo(mw[i]) > 0.0f)) v[2 * i] = 0.0f;
-                            if (!(bf16_hi(mw[i]) > 0.0f)) v[2 * i + 1] = 0.0f;
-                        }
-                    }
-                    out[q] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
-                                        pack_bf16(v[6], v[7]));
-                }
-            }
-        }
+        if (ok) store_pixel<COUT, EPI>(a, tile, tid, acc, bias);
         tc::fence_before_sync();
         if (__syncthreads_or(!ok)) {
             failed = true;
@@ -254,6 +263,158 @@ __global__ void __launch_bounds__(kThreads) conv3x3_kernel(const ConvArgs a) {
         tc::fence_after_sync();
         tc::tmem_dealloc(tmem, 32);
     }
+}
+
+// Warp-specialised variant for BF16 inputs, persistent over tiles. Warp 4 (one lane) loads each
+// tile's halo with TMA, one 8 x 10 x 18 box per 8-channel chunk of a 4-D tensor map over the NHWC
+// input (zero fill outside the image), into a ring of kStages halo slots; warp 5 (one lane) issues
+// the tile's MMAs into one of two TMEM accumulators and commits them to the slot's "empty" and the
+// accumulator's "full" barrier; warps 0-3 drain the accumulator (tcgen05.ld), release it and run
+// the epilogue while the next tile's loads and MMAs are in flight.
+constexpr int kStages = 3;
+constexpr int kTmaThreads = 192;
+constexpr int kTmaCols = 64;  // two 32-column accumulators
+
+template <int CIN, int COUT>
+struct TmaConv {
+    static constexpr int KC = CIN / 8;
+    static constexpr int kWeightVecs = 9 * KC * COUT;
+    // TMA destinations start on 128-byte boundaries: chunks 184 pixels (2944 bytes) apart
+    static constexpr int kChunkPx = 184;
+    static constexpr int kHaloVecs = KC * kChunkPx;
+    static constexpr uint32_t kHaloBytes = kHaloVecs * 16;
+    static constexpr uint32_t kTxBytes = KC * kHaloPx * 16;  // bytes the KC boxes deliver
+    static constexpr int kBars = 2 * kStages + 4;
+    static constexpr size_t kSmem =
+        static_cast<size_t>(kWeightVecs + kStages * kHaloVecs) * 16 + kBars * 8 + 16 + 128;
+    static_assert((kChunkPx * 16) % 128 == 0 && (kWeightVecs * 16) % 128 == 0, "128-byte TMA destinations");
+};
+
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(kTmaThreads, 1) conv3x3_tma_kernel(const __grid_constant__ CUtensorMap in_map,
+                                                                  const ConvArgs a) {
+    using S = TmaConv<CIN, COUT>;
+    constexpr uint32_t kIdesc = tc::instr_desc_bf16(kTilePx, COUT, false, false);
+    static_assert(COUT <= kTmaCols / 2, "two accumulators");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint4* w_s = reinterpret_cast<uint4*>(smem_raw + ((128u - (tc::smem_u32(smem_raw) & 127u)) & 127u));
+    uint4* halo = w_s + S::kWeightVecs;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(halo + kStages * S::kHaloVecs);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + S::kBars);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // barriers: full[s], empty[s] (halo slots), acc_full[k], acc_empty[k] (accumulators)
+    const uint32_t bar0 = tc::smem_u32(bars);
+#define SGS_FULL(st) (bar0 + 8u * (st))
+#define SGS_EMPTY(st) (bar0 + 8u * (kStages + (st)))
+#define SGS_ACC_FULL(k) (bar0 + 8u * (2 * kStages + (k)))
+#define SGS_ACC_EMPTY(k) (bar0 + 8u * (2 * kStages + 2 + (k)))
+
+    for (int i = tid; i < S::kWeightVecs; i += kTmaThreads) w_s[i] = __ldg(a.weights + i);
+    tc::fence_async_smem();
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(slot), kTmaCols);
+    if (tid == 0) {
+        for (int st = 0; st < kStages; ++st) {
+            tc::mbar_init(SGS_FULL(st), 1);
+            tc::mbar_init(SGS_EMPTY(st), 1);
+        }
+        for (int k = 0; k < 2; ++k) {
+            tc::mbar_init(SGS_ACC_FULL(k), 1);
+            tc::mbar_init(SGS_ACC_EMPTY(k), 4);
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    const uint32_t halo_a = tc::smem_u32(halo);
+    const uint32_t w_a = tc::smem_u32(w_s);
+    bool failed = false;
+    int issued = 0;  // producer: tiles whose loads were issued; MMA: tiles whose MMAs were committed
+
+    if (warp == 4) {
+        if (lane == 0) {
+            for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++issued) {
+                const int st = issued % kStages;
+                const uint32_t ph = (issued / kStages) & 1u;
+                if (issued >= kStages && !tc::mbar_wait(SGS_EMPTY(st), ph ^ 1u, kWaitLimit)) {
+                    failed = true;
+                    break;
+                }
+                const TileXY tile = tile_xy(t, a.tiles_x, a.tiles_y);
+                tc::mbar_arrive_expect_tx(SGS_FULL(st), S::kTxBytes);
+#pragma unroll
+                for (int c = 0; c < S::KC; ++c)
+                    tc::tma_load_4d(halo_a + (st * S::kHaloVecs + c * S::kChunkPx) * 16, &in_map, SGS_FULL(st), c * 8,
+                                    tile.x0 - 1, tile.y0 - 1, tile.b);
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {
+            for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++issued) {
+                const int st = issued % kStages, k = issued & 1;
+                const uint32_t ph = (issued / kStages) & 1u, aph = (issued >> 1) & 1u;
+                if (!tc::mbar_wait(SGS_FULL(st), ph, kWaitLimit) ||
+                    (issued >= 2 && !tc::mbar_wait(SGS_ACC_EMPTY(k), aph ^ 1u, kWaitLimit))) {
+                    failed = true;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t h = halo_a + st * S::kHaloBytes;
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap) {
+#pragma unroll
+                    for (int j = 0; j < S::KC / 2; ++j) {
+                        const uint32_t a_addr = h + ((2 * j) * S::kChunkPx + (tap / 3) * kHaloW + tap % 3) * 16;
+                        const uint32_t b_addr = w_a + ((tap * S::KC + 2 * j) * COUT) * 16;
+                        tc::mma_bf16(tmem + k * (kTmaCols / 2), tc::smem_desc(a_addr, S::kChunkPx * 16, kHaloW * 16),
+                                     tc::smem_desc(b_addr, COUT * 16, 128), kIdesc, (tap | j) != 0 ? 1u : 0u);
+                    }
+                }
+                tc::commit(SGS_EMPTY(st));
+                tc::commit(SGS_ACC_FULL(k));
+            }
+        }
+    } else {
+        float bias[COUT];
+#pragma unroll
+        for (int n = 0; n < COUT; ++n) bias[n] = (EPI == kEpiMask) ? 0.0f : __ldg(a.bias + n);
+        int i = 0;
+        for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++i) {
+            const int k = i & 1;
+            const bool ok = __all_sync(0xFFFFFFFFu, tc::mbar_wait(SGS_ACC_FULL(k), (i >> 1) & 1u, kWaitLimit));
+            if (!ok) {
+                failed = true;
+                break;
+            }
+            tc::fence_after_sync();
+            float acc[COUT];
+            load_accumulator<COUT>(tmem + (static_cast<uint32_t>(warp * 32) << 16) + k * (kTmaCols / 2), acc);
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(SGS_ACC_EMPTY(k));
+            store_pixel<COUT, EPI>(a, tile_xy(t, a.tiles_x, a.tiles_y), tid, acc, bias);
+        }
+    }
+
+    if (__syncthreads_or(failed)) {
+        if (tid == 0) atomicExch(&g_error, 1u);
+        // let this CTA's own copies and MMAs in flight finish (bounded) before its memory goes away
+        if (warp == 4 && lane == 0)
+            for (int q = issued - 1; q >= 0 && q >= issued - kStages; --q)
+                tc::mbar_wait(SGS_FULL(q % kStages), (q / kStages) & 1u, kWaitLimit);
+        if (warp == 5 && lane == 0 && issued > 0)
+            tc::mbar_wait(SGS_ACC_FULL((issued - 1) & 1), ((issued - 1) >> 1) & 1u, kWaitLimit);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, kTmaCols);
+    }
+#undef SGS_FULL
+#undef SGS_EMPTY
+#undef SGS_ACC_FULL
+#undef SGS_ACC_EMPTY
 }
 
 // Weight-gradient geometry: im2col groups of 8 rows, (tap, chunk) for tap-major order, then the
@@ -443,7 +604,7 @@ int sm_count() {
 // and threads; at most `cap`. (The occupancy query answers for the default carveout, which keeps
 // these small-footprint kernels at one CTA per SM.)
 template <typename Kernel>
-int resident_ctas(Kernel kernel, size_t smem, int cap) {
+int resident_ctas(Kernel kernel, size_t smem, int cap, int threads = kThreads) {
     int dev = 0, smem_sm = 0, regs_sm = 0;
     cudaFuncAttributes attr{};
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
@@ -456,9 +617,9 @@ int resident_ctas(Kernel kernel, size_t smem, int cap) {
         return 0;
     const size_t per_cta = smem + attr.sharedSizeBytes + 1024;  // 1 KB reserved per CTA
     int blocks = static_cast<int>(static_cast<size_t>(smem_sm) / per_cta);
-    const int regs = attr.numRegs > 0 ? attr.numRegs * kThreads : 1;
+    const int regs = attr.numRegs > 0 ? attr.numRegs * threads : 1;
     if (regs_sm / regs < blocks) blocks = regs_sm / regs;
-    if (2048 / kThreads < blocks) blocks = 2048 / kThreads;
+    if (2048 / threads < blocks) blocks = 2048 / threads;
     return blocks < cap ? blocks : cap;
 }
 
@@ -470,6 +631,50 @@ cudaError_t launch_conv(const ConvArgs& a, cudaStream_t stream) {
     if (per_sm <= 0) return cudaErrorInvalidConfiguration;
     const int grid = a.n_tiles < sm_count() * per_sm ? a.n_tiles : sm_count() * per_sm;
     kernel<<<grid, kThreads, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up through the runtime (no libcuda link).
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 4-D map over a BF16 NHWC tensor [batch][height][width][channels] with a box of 8 channels x the
+// 10 x 18 halo x 1 image.
+bool nhwc_halo_map(CUtensorMap* map, const void* base, int batch, int height, int width, int channels) {
+    const auto fn = encode_tiled();
+    if (fn == nullptr) return false;
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(channels), static_cast<cuuint64_t>(width),
+                                static_cast<cuuint64_t>(height), static_cast<cuuint64_t>(batch)};
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(channels) * 2,
+                                   static_cast<cuuint64_t>(width) * channels * 2,
+                                   static_cast<cuuint64_t>(height) * width * channels * 2};
+    const cuuint32_t box[4] = {8, kHaloW, kHaloH, 1};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, elem,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int CIN, int COUT, int EPI>
+cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t stream) {
+    using S = TmaConv<CIN, COUT>;
+    auto kernel = conv3x3_tma_kernel<CIN, COUT, EPI>;
+    static const int per_sm = resident_ctas(kernel, S::kSmem, 512 / kTmaCols, kTmaThreads);
+    if (per_sm <= 0) return cudaErrorInvalidConfiguration;
+    CUtensorMap map;
+    if (!nhwc_halo_map(&map, a.in, a.batch, a.height, a.width, CIN)) return cudaErrorInvalidValue;
+    const int grid = a.n_tiles < sm_count() * per_sm ? a.n_tiles : sm_count() * per_sm;
+    kernel<<<grid, kTmaThreads, S::kSmem, stream>>>(map, a);
     return cudaGetLastError();
 }
 
@@ -543,13 +748,13 @@ int sgs_conv3x3(const sgs_conv3x3_args* p, void* stream_ptr) {
     if (ci == 8 && co == 32 && epi == SGS_CONV_RELU)
         err = launch_conv<16, 32, kInFeatures, kEpiRelu>(a, stream);
     else if (ci == 32 && co == 32 && epi == SGS_CONV_RELU)
-        err = launch_conv<32, 32, kInBf16, kEpiRelu>(a, stream);
+        err = launch_conv_tma<32, 32, kEpiRelu>(a, stream);
     else if (ci == 32 && co == 16 && epi == SGS_CONV_FINAL)
-        err = launch_conv<32, 16, kInBf16, kEpiFinal>(a, stream);
+        err = launch_conv_tma<32, 16, kEpiFinal>(a, stream);
     else if (ci == 32 && co == 32 && epi == SGS_CONV_MASK)
-        err = launch_conv<32, 32, kInBf16, kEpiMask>(a, stream);
+        err = launch_conv_tma<32, 32, kEpiMask>(a, stream);
     else if (ci == 16 && co == 32 && epi == SGS_CONV_MASK)
-        err = launch_conv<16, 32, kInBf16, kEpiMask>(a, stream);
+        err = launch_conv_tma<16, 32, kEpiMask>(a, stream);
     else
         return record_error(SGS_ERROR_INVALID_ARGUMENT, "conv3x3: unsupported shape %d -> %d, epilogue %d", ci, co,
                             epi);
