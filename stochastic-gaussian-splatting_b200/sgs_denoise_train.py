@@ -3,7 +3,8 @@
 Training data: 2000 pairs at 512 x 512 from 6M-Gaussian scenes drawn like the batched-throughput
 scene (means U[-10, 10]^3, log-scales N(-4.5, 0.8^2), opacity logits N(0, 2^2), SH degree 3) with
 seeds 1..50, 40 random views each (camera 14..30 units from a point within 3 units of the origin,
-60 degree field of view). Each pair holds the features of the first 4, 16, 64 and 256 stochastic-
+with the focal length in pixels of the 60-degree 1080p evaluation camera, a 30.6-degree field of
+view at 512 x 512, so that Gaussians cover as many pixels as in the evaluated frames). Each pair holds the features of the first 4, 16, 64 and 256 stochastic-
 transparency samples and the 1024-sample average as the target. The denoiser trains on random
 128 x 128 crops with an MSE loss (Adam), through the BF16 tensor-core kernels; each crop's input
 sample count is drawn from the four.
@@ -11,7 +12,7 @@ sample count is drawn from the four.
 Evaluation: the seed-0 scene at 1920 x 1080 from views on the radius-25 orbit. The ground truth is
 the 4096-sample average (frames disjoint from the evaluated ones); plain = the progressive average
 of k samples, learned = the denoiser applied to the features of the same k samples, for k in 4, 16,
-64, 256. PSNR (peak 1) and SSIM on premultiplied RGB. Equal-PSNR time: the smallest k at which the
+32, 64, 128, 256. PSNR (peak 1) and SSIM on premultiplied RGB. Equal-PSNR time: the smallest k at which the
 learned resolve reaches the PSNR of the plain 256-sample average, and its render + denoise time
 against 256 plain samples.
 
@@ -40,7 +41,10 @@ TRAIN_RES = 512
 INPUT_SPP = (4, 16, 64, 256)
 TARGET_SPP = 1024
 DEPTH_SCALE = 1.0 / 32.0
-EVAL_SPP = (4, 16, 64, 256)
+EVAL_SPP = (4, 16, 32, 64, 128, 256)
+# training views use the focal length (in pixels) of the 60-degree 1080p evaluation camera, so that
+# Gaussians cover as many pixels in the crops as in the evaluated frames
+EVAL_FOCAL = 540.0 / math.tan(math.radians(30.0))
 GT_SPP = 4096
 
 
@@ -55,7 +59,8 @@ def random_view(gen: torch.Generator, res: int) -> sgs_scenes.Camera:
     radius = 14.0 + 16.0 * float(torch.rand(1, generator=gen, dtype=torch.float64))
     target = (torch.rand(3, generator=gen, dtype=torch.float64) * 6.0 - 3.0)
     pos = target + radius * d
-    return sgs_scenes.pinhole(tuple(float(v) for v in pos), res, res, 60.0, target=tuple(float(v) for v in target))
+    fov = math.degrees(2.0 * math.atan(0.5 * res / EVAL_FOCAL))
+    return sgs_scenes.pinhole(tuple(float(v) for v in pos), res, res, fov, target=tuple(float(v) for v in target))
 
 
 class _Prefetch:
