@@ -237,6 +237,12 @@ int sgs_denoise_status(void* stream);
  * NULL, NULL disables the recording. */
 void sgs_set_stage_events(void* accumulate_start, void* accumulate_end);
 
+/* Diagnostics (no counterpart in the reference): caps the stochastic-transparency large-Gaussian
+ * work queue at `max_entries` entries (0 restores the default, min(N, 2^18)) for the workspace
+ * sizes and renders that follow, process-wide. Gaussians that find the queue full are rendered in
+ * place by their warp (same framebuffer); tests use a small cap to exercise that path. */
+void sgs_set_queue_limit(uint32_t max_entries);
+
 /* Process-wide frame index (render.cu:56-57 keeps it in a hidden static counter that starts at 0);
  * exposed so that random streams can be pinned and resumed. */
 uint32_t sgs_get_frame_index(void);

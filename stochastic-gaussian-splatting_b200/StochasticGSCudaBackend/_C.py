@@ -72,6 +72,12 @@ def set_stage_events(start=None, end=None) -> None:
     _lib.sgs_set_stage_events(start, end)
 
 
+def set_queue_limit(max_entries: int = 0) -> None:
+    """Caps the large-Gaussian work queue of stochastic transparency (0: default); a testing aid for
+    the in-place path taken by Gaussians that find the queue full."""
+    _lib.sgs_set_queue_limit(int(max_entries))
+
+
 def _check(cond: bool, msg: str) -> None:
     if not cond:
         raise RuntimeError(msg)

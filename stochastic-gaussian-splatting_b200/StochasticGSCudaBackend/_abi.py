@@ -148,6 +148,7 @@ SIGNATURES = {
                                    ctypes.c_void_p]),
     "sgs_denoise_status": (ctypes.c_int, [ctypes.c_void_p]),
     "sgs_set_stage_events": (None, [ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_set_queue_limit": (None, [ctypes.c_uint32]),
     "sgs_get_frame_index": (ctypes.c_uint32, []),
     "sgs_set_frame_index": (None, [ctypes.c_uint32]),
     "sgs_k_buffer_size": (ctypes.c_uint32, []),

@@ -7,16 +7,19 @@
 // pixel) and the merge is a minimum, so the result does not depend on which thread evaluates
 // which fragment. This file uses that freedom for a B200-oriented schedule:
 //
-//  * rows, then spans: a warp expands its 32 Gaussians into AABB rows, each lane computes the
-//    conservative x-span of the alpha >= 1/255 ellipse on one row (the AABB corners, ~45% of
-//    its pixels, are never evaluated), and the span pixels of 32 rows are laid end to end
-//    across the lanes, so every lane evaluates one pixel per step whatever the footprint sizes;
-//    the owner of a position is found with one redux.sync OR over the starts and a popc;
-//  * a device-side work queue for Gaussians covering more than kBigFragments pixels: their rows
-//    are cut into chunks that a persistent kernel steals across all SMs (no cross-warp tail,
-//    no host synchronisation);
-//  * u64 atomicMin (fire-and-forget RED) on the L2-resident framebuffer; consecutive lanes hit
-//    consecutive pixels of a row, so each RED touches few L2 sectors.
+//  * rows, then spans: a warp expands its 32 Gaussians into AABB rows, 32 rows at a time, and each
+//    lane computes the conservative x-span of the alpha >= 1/255 ellipse on its row (the AABB
+//    corners, ~45% of its pixels, are never evaluated);
+//  * each lane then walks its own row two pixels per step, the alpha exponent of both pixels in
+//    packed FP32x2 instructions (fma/mul/sub .f32x2 of sm_100a, each element rounded like the scalar
+//    instruction), with no per-pixel owner lookup or shared-memory traffic; the warp steps as often
+//    as its longest row needs, and each accepted pixel issues one predicated RED;
+//  * a device-side work queue for Gaussians covering more than kBigFragments pixels: their rows are
+//    cut into chunks of about kChunkPixels pixels that a persistent kernel steals across all SMs (no
+//    cross-warp tail, no host synchronisation). A chunk has R rows (a power of two <= 32) and each
+//    row is split into 32 / R segments, one lane per segment, so wide footprints keep every lane
+//    walking;
+//  * u64 atomicMin (fire-and-forget RED) on the L2-resident framebuffer.
 //
 // Bit-exactness. The reference's alpha exponent `dx * (cx * dx + cy * dy) + cz * dy * dy` is
 // contracted into fused multiply-adds differently by its scatter loops and by its hybrid gather
@@ -38,15 +41,15 @@ constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kFullMask = 0xffffffffu;
 // Gaussians whose AABB exceeds this many pixels go to the work queue.
 constexpr uint32_t kBigFragments = 2048;
-// Target pixels per stolen chunk (whole rows; a single row wider than this is one chunk).
-constexpr uint32_t kChunkFragments = 2048;
+// Pixels per stolen chunk of a queued Gaussian (whole rows, at most 32 of them).
+constexpr uint32_t kChunkPixels = 2048;
 constexpr uint32_t kQueueBlocksPerSM = 8;
 // Hybrid scheduling: AABBs above this many pixels are gathered by the reference (accumulate_hybrid.cu:26).
 constexpr uint32_t kBinningPixelThreshold = 512;
 // Safety margins of the row spans: exponent units (log2 of alpha) and pixels.
 constexpr float kSpanExpMargin = 0.125f;
 constexpr float kSpanPixelMargin = 0.02f;
-// Flag in RowSlot::c.w: evaluate with the hybrid gather's contraction.
+// Flag in RowGaussian::flags: evaluate with the hybrid gather's contraction.
 constexpr uint32_t kGatherFormFlag = 0x80000000u;
 
 // Per-Gaussian constants of the row/span expansion (64 bytes, four 16-byte words).
@@ -99,130 +102,183 @@ __device__ __forceinline__ uint32_t warp_inclusive_sum(uint32_t v, const uint32_
     return v;
 }
 
-// One row of span pixels ready for evaluation (48 bytes).
-struct RowSlot {
-    float4 a;  // mx, cx, cy * dy, cz * dy
-    uint4 b;   // x offset (first x - first position), row base index (y * width), row seed / blue-noise row, dy bits
-    uint4 c;   // opacity bits, key low, key high, blue-noise x offset | kGatherFormFlag
-};
+// Packed FP32x2 arithmetic (sm_100a): two independent round-to-nearest operations per instruction,
+// bit-identical to the scalar __fsub_rn / __fmul_rn / __fmaf_rn of each element.
+__device__ __forceinline__ unsigned long long f2_pack(const float lo, const float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 f2_unpack(const unsigned long long r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ unsigned long long f2_fma(const unsigned long long a, const unsigned long long b,
+                                                     const unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2_mul(const unsigned long long a, const unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2_add(const unsigned long long a, const unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2_sub(const unsigned long long a, const unsigned long long b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
 
-// Evaluates flattened position p (< total) of the row `r` that owns it (scatter_utils.cuh:35-46).
-// Positions past the end evaluate a valid pixel of the same row and do not merge.
-template <bool kBlue, bool kHybrid>
-__device__ __forceinline__ void st_position(const AccumulateParams& a, const FrameRng& rng, const RowSlot& r,
-                                            const uint32_t p, const uint32_t total) {
-    const float4 ra = r.a;
-    const uint4 rb = r.b;
-    const uint4 rc = r.c;
-    const bool in_range = p < total;
-    const uint32_t x = (in_range ? p : total - 1u) + rb.x;
-    const float dx = __fsub_rn(static_cast<float>(x), ra.x);
-    const float rdy = __uint_as_float(rb.w);
-    const float inner = __fmaf_rn(ra.y, dx, ra.z);
-    float e = __fmaf_rn(ra.w, rdy, __fmul_rn(dx, inner));
-    if (kHybrid && (rc.w & kGatherFormFlag)) e = __fmaf_rn(dx, inner, __fmul_rn(ra.w, rdy));
-    const float alpha = __fmul_rn(__uint_as_float(rc.x), exp2f(fminf(e, 0.0f)));
-    float u;
+// Bits of 1 + u for the white-noise threshold u of pixel x on a row with seed
+// gaussian ^ frame * 1973 ^ y * 2699 (pcg_hash of math_utils.h:113-122; ((w >> 22) ^ w) >> 9 is
+// written as (w >> 9) ^ (w >> 31)).
+__device__ __forceinline__ uint32_t st_threshold_bits(const uint32_t row_seed, const uint32_t x) {
+    const uint32_t state = (row_seed ^ (x * 9277u)) * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return 0x3f800000u | ((word >> 9u) ^ (word >> 31u));
+}
+
+// Blue-noise threshold of pixel x on a row whose slice row starts at texel `row_texel`, with the
+// Gaussian's x offset bx (math_utils.h:125-136).
+__device__ __forceinline__ float st_blue_threshold(const FrameRng& rng, const uint32_t row_texel, const uint32_t x,
+                                                   const uint32_t bx) {
+    const uint32_t texel = row_texel + ((x + bx) % kBlueNoiseWidth);
+    const uint32_t value = (static_cast<uint32_t>(rng.slice[texel]) << 24u) + (1u << 23u) + rng.rotation;
+    return static_cast<float>(value >> 8u) * 5.9604644775390625e-8f;
+}
+
+// Per-row random-number seed: the white-noise seed of row y, or the blue-noise slice row with the
+// Gaussian's x offset in `bx` (math_utils.h:119-136).
+template <bool kBlue>
+__device__ __forceinline__ uint32_t row_seed(const FrameRng& rng, const uint32_t key_lo, const uint32_t y,
+                                             uint32_t& bx) {
     if (kBlue) {
-        const uint32_t texel = rb.z + ((x + (rc.w & 0x7fu)) % kBlueNoiseWidth);
-        const uint32_t value =
-            (static_cast<uint32_t>(rng.slice[texel]) << 24u) + (1u << 23u) + rng.rotation;
-        u = static_cast<float>(value >> 8u) * 5.9604644775390625e-8f;
-    } else {
-        u = __uint_as_float(0x3f800000u | (pcg_hash(rb.z ^ (x * 9277u)) >> 9u)) - 1.0f;
+        const uint32_t oy = (key_lo * 0x91E10DA5u) >> 25u;
+        bx = (key_lo * 0xC13FA9A9u) >> 25u;
+        return ((y + oy) % kBlueNoiseHeight) * kBlueNoiseWidth;
     }
-    if (in_range && alpha >= kMinAlpha && u < alpha) {
-        const unsigned long long key = (static_cast<unsigned long long>(rc.z) << 32) | rc.y;
-        atomicMin(&a.framebuffer[rb.y + x], key);
+    bx = 0;
+    return key_lo ^ (rng.frame * 1973u) ^ (y * 2699u);
+}
+
+// Conservative span [xs, xs + len) of the row at offset dy from the shifted mean, inside the AABB
+// columns; clamped in floating point first, since the ellipse may lie far outside the integer range
+// of the AABB (a non-finite bound leaves the whole AABB row, which is still a superset).
+__device__ __forceinline__ void row_span(const RowGaussian& G, const float dy, uint32_t& xs, uint32_t& len) {
+    const float lo_f = static_cast<float>(G.x_min);
+    const float hi_f = static_cast<float>(G.x_min + G.w - 1u);
+    float fl = lo_f, fh = hi_f;
+    if (G.k2 > 0.0f) {
+        const float rem = fmaf(-dy, dy, G.dymax2);
+        const float hw = sqrtf(G.k2 * fmaxf(rem, 0.0f));
+        const float c = fmaf(G.slope, dy, G.mx);
+        const float eps = kSpanPixelMargin + 4.0e-6f * (fabsf(c) + hw);
+        fl = fmaxf(ceilf(c - hw - eps), lo_f);
+        fh = fminf(floorf(c + hw + eps), hi_f);
+        if (rem < 0.0f) fh = fl - 1.0f;
+    }
+    xs = 0;
+    len = 0;
+    if (fh >= fl) {
+        xs = static_cast<uint32_t>(fl);
+        len = static_cast<uint32_t>(fh) - xs + 1u;
     }
 }
 
-// Each lane holds one row (valid) of Gaussian G at image row y. Computes the spans, lays the span
-// pixels of the 32 rows end to end and evaluates them with all lanes (scatter_utils.cuh:35-46).
+// One predicated 64-bit RED.MIN (no branch around it).
+__device__ __forceinline__ void red_min_if(unsigned long long* address, const unsigned long long key, const bool pred) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p red.relaxed.gpu.global.min.u64 [%0], %1;\n\t}" ::"l"(address),
+        "l"(key), "r"(static_cast<uint32_t>(pred))
+        : "memory");
+}
+
+// Each lane walks segment `seg` of `1 << log_segs` equal parts of the span of its row y (when
+// valid), two pixels per step; the warp takes as many steps as its longest segment needs
+// (scatter_utils.cuh:35-46 per pixel).
 template <bool kBlue, bool kHybrid>
-__device__ __forceinline__ void scatter_rows(const AccumulateParams& a, const FrameRng& rng, const uint32_t lane,
-                                             const uint32_t lt_mask, const uint32_t upto_mask, RowSlot* s_rows,
-                                             const bool valid, const RowGaussian& G, const uint32_t y) {
+__device__ __forceinline__ void walk_rows(const AccumulateParams& a, const FrameRng& rng, const bool valid,
+                                          const RowGaussian& G, const uint32_t y, const uint32_t seg = 0,
+                                          const uint32_t log_segs = 0) {
     uint32_t xs = 0, len = 0;
-    float dy = 0.0f, cydy = 0.0f, czdy = 0.0f;
+    float dy = 0.0f;
     if (valid) {
         dy = __fsub_rn(static_cast<float>(y), G.my);
-        cydy = __fmul_rn(G.cy, dy);
-        czdy = __fmul_rn(G.cz, dy);
-        int lo = static_cast<int>(G.x_min);
-        int hi = static_cast<int>(G.x_min + G.w) - 1;
-        if (G.k2 > 0.0f) {
-            const float rem = fmaf(-dy, dy, G.dymax2);
-            if (rem < 0.0f) {
-                hi = lo - 1;
-            } else {
-                const float hw = sqrtf(G.k2 * rem);
-                const float c = fmaf(G.slope, dy, G.mx);
-                const float eps = kSpanPixelMargin + 4.0e-6f * (fabsf(c) + hw);
-                const float fl = ceilf(c - hw - eps);
-                const float fh = floorf(c + hw + eps);
-                // compare in float first: the span may lie far outside the int range of the AABB
-                if (fl > static_cast<float>(hi) || fh < static_cast<float>(lo)) {
-                    hi = lo - 1;
-                } else {
-                    if (fl > static_cast<float>(lo)) lo = static_cast<int>(fl);
-                    if (fh < static_cast<float>(hi)) hi = static_cast<int>(fh);
-                }
-            }
-        }
-        if (hi >= lo) {
-            xs = static_cast<uint32_t>(lo);
-            len = static_cast<uint32_t>(hi - lo + 1);
+        row_span(G, dy, xs, len);
+        if (log_segs > 0) {
+            const uint32_t part = (len + (1u << log_segs) - 1u) >> log_segs;
+            const uint32_t skip = min(seg * part, len);
+            xs += skip;
+            len = min(len - skip, part);
         }
     }
-    // compact the non-empty rows into shared memory, in lane order
-    const uint32_t rmask = __ballot_sync(kFullMask, len > 0);
-    if (rmask == 0) return;
-    const uint32_t incl = warp_inclusive_sum(len, lane);
-    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-    const uint32_t first = incl - len;
-    if (len > 0) {
-        const uint32_t slot = __popc(rmask & lt_mask);
-        uint32_t seed, bx = 0;
+    const uint32_t steps = __reduce_max_sync(kFullMask, len);
+    if (steps == 0) return;
+    const float cydy = __fmul_rn(G.cy, dy);
+    const float czdy = __fmul_rn(G.cz, dy);
+    uint32_t bx;
+    const uint32_t seed = row_seed<kBlue>(rng, G.key_lo, y, bx);
+    const unsigned long long key = (static_cast<unsigned long long>(G.key_hi) << 32) | G.key_lo;
+    const bool gather_form = kHybrid && (G.flags & kGatherFormFlag);
+    unsigned long long* row = a.framebuffer + (static_cast<size_t>(y) * a.cam.width_int + xs);
+    const unsigned long long mx2 = f2_pack(G.mx, G.mx), cx2 = f2_pack(G.cx, G.cx), cydy2 = f2_pack(cydy, cydy);
+    const unsigned long long czdy2 = f2_pack(czdy, czdy), dy2 = f2_pack(dy, dy);
+    const unsigned long long opacity2 = f2_pack(G.opacity, G.opacity);
+    const unsigned long long two = f2_pack(2.0f, 2.0f);
+    const float fxs = static_cast<float>(xs);  // pixel coordinates are exact in float
+    unsigned long long fx = f2_pack(fxs, fxs + 1.0f);
+    for (uint32_t i = 0; i < steps; i += 2) {
+        // alpha of pixels xs + i and xs + i + 1 with the reference's contraction of the exponent
+        const unsigned long long dx = f2_sub(fx, mx2);
+        const unsigned long long inner = f2_fma(cx2, dx, cydy2);
+        const unsigned long long e2 =
+            gather_form ? f2_fma(dx, inner, f2_mul(czdy2, dy2)) : f2_fma(czdy2, dy2, f2_mul(dx, inner));
+        const float2 e = f2_unpack(e2);
+        const float2 alpha =
+            f2_unpack(f2_mul(opacity2, f2_pack(exp2f(fminf(e.x, 0.0f)), exp2f(fminf(e.y, 0.0f)))));
+        const uint32_t x0 = xs + i;
+        float2 u;
         if (kBlue) {
-            const uint32_t oy = (G.key_lo * 0x91E10DA5u) >> 25u;
-            bx = (G.key_lo * 0xC13FA9A9u) >> 25u;
-            seed = ((y + oy) % kBlueNoiseHeight) * kBlueNoiseWidth;
+            u = make_float2(st_blue_threshold(rng, seed, x0, bx), st_blue_threshold(rng, seed, x0 + 1u, bx));
         } else {
-            seed = G.key_lo ^ (rng.frame * 1973u) ^ (y * 2699u);
+            u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed, x0)),
+                                         __uint_as_float(st_threshold_bits(seed, x0 + 1u))),
+                                 f2_pack(1.0f, 1.0f)));
         }
-        RowSlot r;
-        r.a = make_float4(G.mx, G.cx, cydy, czdy);
-        r.b = make_uint4(xs - first, y * a.cam.width_int, seed, __float_as_uint(dy));
-        r.c = make_uint4(__float_as_uint(G.opacity), G.key_lo, G.key_hi, bx | G.flags);
-        s_rows[slot] = r;
+        red_min_if(row + i, key, i < len && alpha.x >= kMinAlpha && u.x < alpha.x);
+        red_min_if(row + i + 1u, key, i + 1u < len && alpha.y >= kMinAlpha && u.y < alpha.y);
+        fx = f2_add(fx, two);
     }
-    __syncwarp();
-    // two positions per lane and step (p and p + 32): one pass over 64 positions; the body is
-    // straight-line code ending in one predicated RED
-    int prev = -1;
-    for (uint32_t base = 0; base < total; base += 64) {
-        const uint32_t rel = first - base;
-        const bool starts = len > 0 && rel < 64u;
-        const uint32_t bits_lo = __reduce_or_sync(kFullMask, (starts && rel < 32u) ? (1u << rel) : 0u);
-        const uint32_t bits_hi = __reduce_or_sync(kFullMask, (starts && rel >= 32u) ? (1u << (rel - 32u)) : 0u);
-        const int n_lo = __popc(bits_lo);
-        const int owner0 = prev + __popc(bits_lo & upto_mask);
-        const int owner1 = prev + n_lo + __popc(bits_hi & upto_mask);
-        prev += n_lo + __popc(bits_hi);
-        st_position<kBlue, kHybrid>(a, rng, s_rows[owner0], base + lane, total);
-        st_position<kBlue, kHybrid>(a, rng, s_rows[owner1], base + 32u + lane, total);
-    }
-    __syncwarp();
 }
 
-__device__ __forceinline__ uint32_t rows_per_chunk(const uint32_t w) { return max(1u, kChunkFragments / w); }
+// Rows per chunk of a queued Gaussian of AABB width w: about kChunkPixels pixels, a power of two
+// between 1 and 32; each row of the chunk is walked in 32 / rows segments.
+__device__ __forceinline__ uint32_t log_chunk_rows(const uint32_t w) {
+    const uint32_t rows = max(1u, min(32u, kChunkPixels / max(w, 1u)));
+    return 31u - __clz(rows);
+}
+
+// Rows [r0, r0 + (1 << log_rows)) of G, clipped to r_end: lane l walks segment l >> log_rows of row
+// r0 + (l & (rows - 1)).
+template <bool kBlue, bool kHybrid>
+__device__ __forceinline__ void walk_chunk(const AccumulateParams& a, const FrameRng& rng, const uint32_t lane,
+                                           const RowGaussian& G, const uint32_t r0, const uint32_t log_rows,
+                                           const uint32_t r_end) {
+    const uint32_t r = r0 + (lane & ((1u << log_rows) - 1u));
+    walk_rows<kBlue, kHybrid>(a, rng, r < r_end, G, G.y_min + r, lane >> log_rows, 5u - log_rows);
+}
 
 // One thread per Gaussian (accumulate_scatter.cu:19-77 for the projection and the AABB).
 template <bool kBlue, bool kHybrid>
 __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateParams a) {
     __shared__ RowGaussian s_gauss[kWarpsPerBlock][32];
-    __shared__ RowSlot s_rows[kWarpsPerBlock][32];
 
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t wib = threadIdx.x >> 5;
@@ -274,8 +330,8 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
     bool has_rows = count > 0;
     if (count > kBigFragments) {
         has_rows = false;
-        const uint32_t rpc = rows_per_chunk(rect.width);
-        const uint32_t chunks = (rect.height + rpc - 1) / rpc;
+        const uint32_t log_rpc = log_chunk_rows(rect.width);
+        const uint32_t chunks = (rect.height + (1u << log_rpc) - 1u) >> log_rpc;
         const unsigned long long old = atomicAdd(&a.queue->packed, (1ull << kQueueEntryShift) | chunks);
         const uint32_t e = static_cast<uint32_t>(old >> kQueueEntryShift);
         const unsigned long long first_chunk = old & kQueueChunkMask;
@@ -283,7 +339,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
             a.q.key[e] = key;
             a.q.geom[e] = make_float4(G.mx, G.my, G.cx, G.cy);
             a.q.geom2[e] = make_float4(G.cz, G.opacity, __uint_as_float(rect.x_min), __uint_as_float(rect.width));
-            a.q.meta[e] = make_uint4(rect.y_min, rect.height, rpc | G.flags, static_cast<uint32_t>(first_chunk));
+            a.q.meta[e] = make_uint4(rect.y_min, rect.height, log_rpc | G.flags, static_cast<uint32_t>(first_chunk));
         } else {
             keep_big = true;
             atomicAdd(&a.queue->overflow, 1u);
@@ -312,7 +368,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         const bool valid = r < total_rows;
         const RowGaussian rg = s_gauss[wib][valid ? owner : 0];
         const uint32_t y = rg.y_min + (r - rg.row_first);
-        scatter_rows<kBlue, kHybrid>(a, rng, lane, lt_mask, upto_mask, s_rows[wib], valid, rg, y);
+        walk_rows<kBlue, kHybrid>(a, rng, valid, rg, y);
     }
 
     // queue overflow: the warp processes its kept large Gaussians, 32 rows at a time
@@ -325,29 +381,22 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         if (lane == src) s_gauss[wib][0] = G;
         __syncwarp();
         const RowGaussian bg = s_gauss[wib][0];
-        for (uint32_t r0 = 0; r0 < bh; r0 += 32) {
-            const bool valid = r0 + lane < bh;
-            scatter_rows<kBlue, kHybrid>(a, rng, lane, lt_mask, upto_mask, s_rows[wib], valid, bg, bg.y_min + r0 + lane);
-        }
+        for (uint32_t r0 = 0; r0 < bh; r0 += 32) walk_rows<kBlue, kHybrid>(a, rng, r0 + lane < bh, bg, bg.y_min + r0 + lane);
     }
 }
 
 // Persistent consumer of the large-Gaussian queue: each warp steals one chunk of rows at a time.
 template <bool kBlue, bool kHybrid>
 __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams a) {
-    __shared__ RowSlot s_rows[kWarpsPerBlock][32];
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t wib = threadIdx.x >> 5;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    const uint32_t upto_mask = kFullMask >> (31u - lane);
     const unsigned long long packed = a.queue->packed;
     const FrameRng rng = frame_rng(a);
     const uint32_t n_entries =
         static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(a.q.capacity)));
     if (n_entries == 0) return;
     const uint4 last = a.q.meta[n_entries - 1];
-    const uint32_t last_rpc = last.z & ~kGatherFormFlag;
-    const uint32_t n_chunks = last.w + (last.y + last_rpc - 1) / last_rpc;
+    const uint32_t last_log_rpc = last.z & ~kGatherFormFlag;
+    const uint32_t n_chunks = last.w + ((last.y + (1u << last_log_rpc) - 1u) >> last_log_rpc);
     for (;;) {
         uint32_t c = 0;
         if (lane == 0) c = atomicAdd(&a.queue->next_chunk, 1u);
@@ -379,17 +428,13 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
         G.row_first = 0;
         G.flags = m.z & kGatherFormFlag;
         span_constants(G);
-        const uint32_t rpc = m.z & ~kGatherFormFlag;
-        const uint32_t r0 = (c - m.w) * rpc;
-        if (r0 >= m.y || G.w == 0 || rpc == 0) {
+        const uint32_t log_rpc = m.z & ~kGatherFormFlag;
+        const uint32_t r0 = (c - m.w) << log_rpc;
+        if (r0 >= m.y || G.w == 0 || log_rpc > 5u) {
             if (lane == 0) atomicOr(&a.queue->error, 1u);
             continue;
         }
-        const uint32_t r1 = min(r0 + rpc, m.y);
-        for (uint32_t r = r0; r < r1; r += 32) {
-            const bool valid = r + lane < r1;
-            scatter_rows<kBlue, kHybrid>(a, rng, lane, lt_mask, upto_mask, s_rows[wib], valid, G, G.y_min + r + lane);
-        }
+        walk_chunk<kBlue, kHybrid>(a, rng, lane, G, r0, log_rpc, m.y);
     }
 }
 

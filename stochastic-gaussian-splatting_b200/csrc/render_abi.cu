@@ -24,6 +24,8 @@ thread_local std::string t_last_error;
 // optional accumulate-stage events (sgs_set_stage_events)
 thread_local cudaEvent_t t_stage_start = nullptr;
 thread_local cudaEvent_t t_stage_end = nullptr;
+// optional cap on the stochastic-transparency large-Gaussian queue (sgs_set_queue_limit), 0 = none
+std::atomic<uint32_t> g_queue_limit{0};
 
 constexpr size_t kAlign = 256;
 constexpr uint32_t kDefaultMaxBinned = 1u << 20;     // accumulate_hybrid_gps.cu:22
@@ -86,6 +88,8 @@ int derive(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, D
             if (s->hybrid_scheduling)
                 d.max_binned = std::min(s->max_binned != 0 ? s->max_binned : kDefaultMaxBinned, g->n_gaussians);
             d.queue_capacity = std::min(g->n_gaussians, kStQueueCapacity);
+            const uint32_t cap = g_queue_limit.load(std::memory_order_relaxed);
+            if (cap != 0) d.queue_capacity = std::min(d.queue_capacity, cap);
             const uint64_t limit = 0xffffffffull / std::max<uint64_t>(fbh, 1);
             if (d.queue_capacity > limit) d.queue_capacity = static_cast<uint32_t>(limit);
         }
@@ -313,6 +317,8 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));
     return SGS_OK;
 }
+
+void sgs_set_queue_limit(uint32_t max_entries) { g_queue_limit.store(max_entries, std::memory_order_relaxed); }
 
 void sgs_set_stage_events(void* accumulate_start, void* accumulate_end) {
     t_stage_start = static_cast<cudaEvent_t>(accumulate_start);
