@@ -158,6 +158,27 @@ int sgs_backward_finish(const sgs_gaussians* gaussians, const sgs_camera* camera
                         void* backward_workspace, float* d_means, float* d_scales, float* d_rotations,
                         float* d_opacities, float* d_sh, void* stream);
 
+/* Fused form of step 1 for S samples that share the upstream gradients and the weight (a plain
+ * progressive average: weight = 1/S): one walk over every Gaussian's fragments evaluates alpha and
+ * the geometric factors once and sums the S samples' contributions, instead of S walks.
+ *   a. for each sample s < S: sgs_backward_sample_terms with the workspace of the sgs_render call
+ *      that produced it (or of a re-render with the same frame index), which stores that sample's
+ *      winner and colour term per framebuffer pixel in `scratch`; the workspace may be reused for
+ *      the next sample once this call is enqueued;
+ *   b. sgs_backward_accumulate_samples: the walk; `first` = 1 clears the accumulators.
+ * `scratch` holds sgs_backward_samples_scratch_size(camera, settings, S) bytes (12 bytes per
+ * framebuffer pixel and sample), 256-byte aligned; S is at most 1024. Same estimator, supported
+ * settings and sgs_backward_finish as above. */
+size_t sgs_backward_samples_scratch_size(const sgs_camera* camera, const sgs_settings* settings, uint32_t n_samples);
+int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                              const void* render_workspace, const float* grad_image, const float* grad_alpha,
+                              const float* grad_depth, float weight, uint32_t sample, uint32_t n_samples,
+                              void* scratch, void* stream);
+int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_camera* camera,
+                                    const sgs_settings* settings, const float* grad_image, const float* grad_alpha,
+                                    const float* grad_depth, float weight, uint32_t n_samples, int first,
+                                    void* scratch, void* backward_workspace, void* stream);
+
 /* ---- Learned resolve (no counterpart in the reference) ------------------------------------------
  * A 6-layer 3x3 convolutional denoiser (8 -> 32 -> 32 -> 32 -> 32 -> 32 -> 3, ReLU between layers,
  * the last layer adds the mean colour back) that maps a few samples' features to the converged

@@ -8,8 +8,11 @@ backward pass to all five parameter tensors (the reference renders only; it has 
 The backward is an unbiased estimator of the gradient of the expected image (see
 csrc/backward_st.cu): each sample's winners give a one-sample estimate, averaged over the samples.
 Winners are either kept from the forward pass (`store_winners=True`, 24 bytes per framebuffer pixel
-and sample) or recomputed by rendering the same frame indices again (`store_winners=False`: no
-memory per sample, one more render per sample).
+and sample) or recomputed by rendering the same frame indices again (`store_winners=False`: one more
+render per sample, no render workspace kept per sample). Either way the backward first tabulates
+every sample's winner and colour term (12 bytes per framebuffer pixel and sample) and then walks
+the Gaussians' fragments once for all samples (sgs_backward_sample_terms,
+sgs_backward_accumulate_samples).
 """
 from __future__ import annotations
 
@@ -80,21 +83,30 @@ class _RenderSamples(torch.autograd.Function):
                          device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
         weight = 1.0 / ctx.n_samples
+        n = ctx.n_samples
+        # one table of every sample's winners and colour terms, then one fused walk over the fragments
+        scratch = torch.empty(_lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s), n),
+                              dtype=torch.uint8, device=dev)
+        gptr = [None if t is None else ctypes.c_void_p(t.data_ptr()) for t in grads_in]
         e = torch.empty(0)
         hist = (e, e, e, e)
-        for k in range(ctx.n_samples):
+        for k in range(n):
             if ctx.workspaces:
                 ws = ctx.workspaces[k]
             else:
                 hist, ws, _ = _render_one(tensors, settings, hist, 0 if k == 0 else 1, ctx.first_frame + k)
-            st = _lib.sgs_backward_accumulate(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
-                                              ctypes.c_void_p(ws.data_ptr()), ctypes.c_void_p(grads_in[0].data_ptr()),
-                                              None if grads_in[1] is None else ctypes.c_void_p(grads_in[1].data_ptr()),
-                                              None if grads_in[2] is None else ctypes.c_void_p(grads_in[2].data_ptr()),
-                                              ctypes.c_float(weight), int(k == 0), ctypes.c_void_p(bw.data_ptr()),
-                                              ctypes.c_void_p(stream))
+            st = _lib.sgs_backward_sample_terms(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
+                                                ctypes.c_void_p(ws.data_ptr()), gptr[0], gptr[1], gptr[2],
+                                                ctypes.c_float(weight), k, n, ctypes.c_void_p(scratch.data_ptr()),
+                                                ctypes.c_void_p(stream))
             if st != _abi.SGS_OK:
-                raise RuntimeError(f"sgs_backward_accumulate failed ({st}): {_abi.last_error(_lib)}")
+                raise RuntimeError(f"sgs_backward_sample_terms failed ({st}): {_abi.last_error(_lib)}")
+        st = _lib.sgs_backward_accumulate_samples(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), gptr[0], gptr[1],
+                                                  gptr[2], ctypes.c_float(weight), n, 1,
+                                                  ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(bw.data_ptr()),
+                                                  ctypes.c_void_p(stream))
+        if st != _abi.SGS_OK:
+            raise RuntimeError(f"sgs_backward_accumulate_samples failed ({st}): {_abi.last_error(_lib)}")
         outs = [torch.empty_like(t) for t in tensors]
         st = _lib.sgs_backward_finish(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(bw.data_ptr()),
                                       *(ctypes.c_void_p(t.data_ptr()) for t in outs), ctypes.c_void_p(stream))

@@ -32,6 +32,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "sgs_internal.h"
+#include "sgs_rows.cuh"
 
 namespace sgs {
 namespace {
@@ -46,9 +47,6 @@ constexpr uint32_t kChunkPixels = 2048;
 constexpr uint32_t kQueueBlocksPerSM = 8;
 // Hybrid scheduling: AABBs above this many pixels are gathered by the reference (accumulate_hybrid.cu:26).
 constexpr uint32_t kBinningPixelThreshold = 512;
-// Safety margins of the row spans: exponent units (log2 of alpha) and pixels.
-constexpr float kSpanExpMargin = 0.125f;
-constexpr float kSpanPixelMargin = 0.02f;
 // Flag in RowGaussian::flags: evaluate with the hybrid gather's contraction.
 constexpr uint32_t kGatherFormFlag = 0x80000000u;
 
@@ -58,49 +56,13 @@ struct RowGaussian {
     float cx, cy;       // exp2-scaled conic (x, y)
     float cz;           // exp2-scaled conic z
     float opacity;
-    float slope;        // row centre shift per unit dy
-    float k2;           // squared half-width per unit of (dymax2 - dy^2); 0 disables spans
-    float dymax2;       // rows with dy^2 > dymax2 hold no pixel with alpha >= 1/255
+    SpanConstants span; // conservative row spans (sgs_rows.cuh)
     uint32_t key_lo, key_hi;
     uint32_t x_min;
     uint32_t y_min, w;
     uint32_t row_first; // first row position in the warp's row list (level 1)
     uint32_t flags;     // kGatherFormFlag
 };
-
-// Span constants. For a row at offset dy the exponent is the concave quadratic
-// e(dx) = cx dx^2 + cy dy dx + cz dy^2 with its maximum at dx = slope * dy; pixels with
-// alpha >= 1/255 need e >= T = -log2(255 opacity). Using T minus kSpanExpMargin (far above the
-// float error of e or of these constants, which enter only relative to |T|) and widening by
-// kSpanPixelMargin gives a superset of the accepted pixels of every row.
-__device__ __forceinline__ void span_constants(RowGaussian& G) {
-    const float T = -log2f(G.opacity * kMinAlphaRcp) - kSpanExpMargin;
-    const float P = 4.0f * G.cx * G.cz - G.cy * G.cy;  // > 0 for a positive-definite conic
-    G.slope = 0.0f;
-    G.k2 = 0.0f;
-    G.dymax2 = 0.0f;
-    if (P > 0.0f && G.cx < 0.0f && T < 0.0f) {
-        const float inv_cx = 1.0f / G.cx;
-        const float k2 = 0.25f * P * inv_cx * inv_cx;
-        const float dymax2 = 4.0f * G.cx * T / P;
-        const float slope = -0.5f * G.cy * inv_cx;
-        if (isfinite(k2) && isfinite(dymax2) && isfinite(slope) && k2 > 0.0f) {
-            G.k2 = k2;
-            G.dymax2 = dymax2;
-            G.slope = slope;
-        }
-    }
-}
-
-// Inclusive warp prefix sum.
-__device__ __forceinline__ uint32_t warp_inclusive_sum(uint32_t v, const uint32_t lane) {
-#pragma unroll
-    for (uint32_t o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFullMask, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
 
 // Packed FP32x2 arithmetic (sm_100a): two independent round-to-nearest operations per instruction,
 // bit-identical to the scalar __fsub_rn / __fmul_rn / __fmaf_rn of each element.
@@ -168,30 +130,6 @@ __device__ __forceinline__ uint32_t row_seed(const FrameRng& rng, const uint32_t
     return key_lo ^ (rng.frame * 1973u) ^ (y * 2699u);
 }
 
-// Conservative span [xs, xs + len) of the row at offset dy from the shifted mean, inside the AABB
-// columns; clamped in floating point first, since the ellipse may lie far outside the integer range
-// of the AABB (a non-finite bound leaves the whole AABB row, which is still a superset).
-__device__ __forceinline__ void row_span(const RowGaussian& G, const float dy, uint32_t& xs, uint32_t& len) {
-    const float lo_f = static_cast<float>(G.x_min);
-    const float hi_f = static_cast<float>(G.x_min + G.w - 1u);
-    float fl = lo_f, fh = hi_f;
-    if (G.k2 > 0.0f) {
-        const float rem = fmaf(-dy, dy, G.dymax2);
-        const float hw = sqrtf(G.k2 * fmaxf(rem, 0.0f));
-        const float c = fmaf(G.slope, dy, G.mx);
-        const float eps = kSpanPixelMargin + 4.0e-6f * (fabsf(c) + hw);
-        fl = fmaxf(ceilf(c - hw - eps), lo_f);
-        fh = fminf(floorf(c + hw + eps), hi_f);
-        if (rem < 0.0f) fh = fl - 1.0f;
-    }
-    xs = 0;
-    len = 0;
-    if (fh >= fl) {
-        xs = static_cast<uint32_t>(fl);
-        len = static_cast<uint32_t>(fh) - xs + 1u;
-    }
-}
-
 // One predicated 64-bit RED.MIN (no branch around it).
 __device__ __forceinline__ void red_min_if(unsigned long long* address, const unsigned long long key, const bool pred) {
     asm volatile(
@@ -211,7 +149,7 @@ __device__ __forceinline__ void walk_rows(const AccumulateParams& a, const Frame
     float dy = 0.0f;
     if (valid) {
         dy = __fsub_rn(static_cast<float>(y), G.my);
-        row_span(G, dy, xs, len);
+        row_span(G.x_min, G.w, G.mx, G.span, dy, xs, len);
         if (log_segs > 0) {
             const uint32_t part = (len + (1u << log_segs) - 1u) >> log_segs;
             const uint32_t skip = min(seg * part, len);
@@ -310,7 +248,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
     G.w = rect.width;
     G.row_first = 0;
     G.flags = 0;
-    span_constants(G);
+    G.span = span_constants(G.cx, G.cy, G.cz, G.opacity);
 
     if (kHybrid) {
         // the reference gathers the first min(N, 2^20) Gaussians with more than 512 pixels
@@ -427,7 +365,7 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
         G.y_min = m.x;
         G.row_first = 0;
         G.flags = m.z & kGatherFormFlag;
-        span_constants(G);
+        G.span = span_constants(G.cx, G.cy, G.cz, G.opacity);
         const uint32_t log_rpc = m.z & ~kGatherFormFlag;
         const uint32_t r0 = (c - m.w) << log_rpc;
         if (r0 >= m.y || G.w == 0 || log_rpc > 5u) {

@@ -55,7 +55,20 @@ int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, Ba
     p.cam.proper_aa = false;
     p.width = c->width;
     p.ss = ss;
+    p.n_fb = c->width * ss * c->height * ss;
     return SGS_OK;
+}
+
+constexpr uint32_t kMaxFusedSamples = 1024;
+
+size_t align256(const size_t v) { return (v + 255) & ~size_t(255); }
+
+// Interleaved per-pixel sample table of the fused backward: keys, then terms.
+void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples) {
+    p.n_samples = n_samples;
+    p.pix_keys = static_cast<unsigned long long*>(scratch);
+    p.pix_terms = reinterpret_cast<float*>(static_cast<char*>(scratch) +
+                                           align256(sizeof(unsigned long long) * p.n_fb * static_cast<size_t>(n_samples)));
 }
 
 void set_backward_buffers(BackwardParams& p, void* backward_workspace) {
@@ -99,6 +112,74 @@ int sgs_backward_accumulate(const sgs_gaussians* gaussians, const sgs_camera* ca
         if (err == cudaSuccess) err = launch_backward_colors(p, stream);
     }
     if (err == cudaSuccess) err = launch_backward_fragments(p, stream);
+    if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
+    return SGS_OK;
+}
+
+size_t sgs_backward_samples_scratch_size(const sgs_camera* camera, const sgs_settings* settings,
+                                         uint32_t n_samples) {
+    if (camera == nullptr || settings == nullptr || n_samples == 0 || n_samples > kMaxFusedSamples) return 0;
+    const uint32_t ss = settings->supersampling_factor < 1 ? 1u : static_cast<uint32_t>(settings->supersampling_factor);
+    const size_t n_fb = static_cast<size_t>(camera->width) * ss * camera->height * ss;
+    return align256(sizeof(unsigned long long) * n_fb * n_samples) + align256(sizeof(float) * n_fb * n_samples);
+}
+
+int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                              const void* render_workspace, const float* grad_image, const float* grad_alpha,
+                              const float* grad_depth, float weight, uint32_t sample, uint32_t n_samples,
+                              void* scratch, void* stream_ptr) {
+    BackwardSetup S;
+    int st = setup(gaussians, camera, settings, S);
+    if (st != SGS_OK) return st;
+    if (render_workspace == nullptr || grad_image == nullptr || scratch == nullptr ||
+        (reinterpret_cast<uintptr_t>(scratch) & 255u) != 0)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT,
+                            "null render workspace or image gradient, or scratch not 256-byte aligned");
+    if (n_samples == 0 || n_samples > kMaxFusedSamples || sample >= n_samples)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT, "sample %u of %u (at most %u samples)", sample, n_samples,
+                            kMaxFusedSamples);
+    BackwardParams& p = S.p;
+    const char* ws = static_cast<const char*>(render_workspace);
+    p.framebuffer = reinterpret_cast<const unsigned long long*>(ws + S.layout.framebuffer);
+    p.samples = reinterpret_cast<const float4*>(ws + S.layout.samples);
+    p.grad_image = grad_image;
+    p.grad_alpha = grad_alpha;
+    p.grad_depth = grad_depth;
+    p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
+    set_sample_table(p, scratch, n_samples);
+    p.sample = sample;
+    const cudaError_t err = launch_backward_sample_terms(p, static_cast<cudaStream_t>(stream_ptr));
+    if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
+    return SGS_OK;
+}
+
+int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_camera* camera,
+                                    const sgs_settings* settings, const float* grad_image, const float* grad_alpha,
+                                    const float* grad_depth, float weight, uint32_t n_samples, int first,
+                                    void* scratch, void* backward_workspace, void* stream_ptr) {
+    BackwardSetup S;
+    int st = setup(gaussians, camera, settings, S);
+    if (st != SGS_OK) return st;
+    if (grad_image == nullptr || scratch == nullptr || backward_workspace == nullptr ||
+        (reinterpret_cast<uintptr_t>(scratch) & 255u) != 0 || (reinterpret_cast<uintptr_t>(backward_workspace) & 15u) != 0)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT,
+                            "null image gradient, scratch or backward workspace, or misaligned buffers");
+    if (n_samples == 0 || n_samples > kMaxFusedSamples)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT, "%u samples (1 to %u)", n_samples, kMaxFusedSamples);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    BackwardParams& p = S.p;
+    p.grad_image = grad_image;
+    p.grad_alpha = grad_alpha;
+    p.grad_depth = grad_depth;
+    p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
+    set_sample_table(p, scratch, n_samples);
+    set_backward_buffers(p, backward_workspace);
+    cudaError_t err = cudaSuccess;
+    if (first) {
+        err = cudaMemsetAsync(p.accum, 0, kAccumFloats * p.n * sizeof(float), stream);
+        if (err == cudaSuccess) err = launch_backward_colors(p, stream);
+    }
+    if (err == cudaSuccess) err = launch_backward_fragments_samples(p, stream);
     if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
     return SGS_OK;
 }

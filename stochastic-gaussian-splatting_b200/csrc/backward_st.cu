@@ -18,11 +18,13 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "sgs_internal.h"
+#include "sgs_rows.cuh"
 
 namespace sgs {
 namespace {
 
 constexpr uint32_t kBlock = 256;
+constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kFullMask = 0xffffffffu;
 constexpr uint32_t kCoopFragments = 64;  // larger AABBs are processed by the whole warp
 constexpr int kAccum = 10;               // op, conic x/y/z, mean2d x/y, depth, colour r/g/b
@@ -140,6 +142,205 @@ __global__ void __launch_bounds__(kBlock) fragments_backward_kernel(const Backwa
 #pragma unroll
     for (int i = 0; i < kAccum; ++i)
         if (acc.v[i] != 0.0f) out[i] += acc.v[i];
+}
+
+
+// ---- Fused form over S samples ------------------------------------------------------------------
+// The estimator is a sum over samples of terms that depend on the sample only through the pixel's
+// winner. sample_terms_kernel stores, per framebuffer pixel and sample, the winner key and
+// T = s (g . c_w + g_d z_w); one walk over every Gaussian's fragments then evaluates alpha and the
+// geometric factors once and sums the S samples' contributions:
+//   dL/da_k = ge (g . c_k + g_d z_k) - sum_{key_w > key_k} T / (1 - a_k) + g_a n_none / (1 - a_k)
+// with ge = #samples whose winner is not in front of k and n_none = #samples with no winner.
+
+__global__ void __launch_bounds__(kBlock) sample_terms_kernel(const BackwardParams b) {
+    const uint32_t pix = blockIdx.x * kBlock + threadIdx.x;
+    if (pix >= b.n_fb) return;
+    const unsigned long long key = b.framebuffer[pix];
+    const float4 sw = b.samples[pix];  // winner colour and depth (0 for background)
+    const uint32_t px = pix % b.cam.width_int, py = pix / b.cam.width_int;
+    const uint32_t ip = (py / b.ss) * b.width + px / b.ss;
+    float t = b.grad_image[3 * ip + 0] * sw.x + b.grad_image[3 * ip + 1] * sw.y + b.grad_image[3 * ip + 2] * sw.z;
+    if (b.grad_depth != nullptr) t += b.grad_depth[ip] * sw.w;
+    const size_t slot = static_cast<size_t>(pix) * b.n_samples + b.sample;
+    b.pix_keys[slot] = key;
+    b.pix_terms[slot] = t * b.grad_scale;
+}
+
+// Per-Gaussian constants of the fused walk (96 bytes).
+struct WalkGaussian {
+    float mx, my;             // mean2d - 0.5
+    float cx, cy, cz;         // exp2-scaled conic
+    float opacity;
+    SpanConstants span;
+    float conic_x, conic_y, conic_z;
+    float depth;
+    float ckx, cky, ckz;      // view-dependent colour
+    uint32_t key_lo, key_hi;
+    uint32_t x_min, y_min, w;
+    uint32_t row_first;       // first row position in the warp's row list
+    uint32_t pad[2];
+};
+
+// Lane walks the span of row y of Gaussian q (when valid), one pixel per step, and adds the S
+// samples' fragment gradients to acc.
+__device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, const WalkGaussian& q, const bool valid,
+                                                   const uint32_t y, FragAccum& acc) {
+    uint32_t xs = 0, len = 0;
+    float dy = 0.0f;
+    if (valid) {
+        dy = static_cast<float>(y) - q.my;
+        row_span(q.x_min, q.w, q.mx, q.span, dy, xs, len);
+    }
+    const uint32_t steps = __reduce_max_sync(kFullMask, len);
+    if (steps == 0) return;
+    const uint32_t S = b.n_samples;
+    const float gs = b.grad_scale;
+    const float cydy = q.cy * dy, czdy = q.cz * dy;
+    const uint32_t iy = y / b.ss;
+    const float* g_row = b.grad_image + 3 * static_cast<size_t>(iy) * b.width;
+    const float* ga_row = b.grad_alpha != nullptr ? b.grad_alpha + static_cast<size_t>(iy) * b.width : nullptr;
+    const float* gd_row = b.grad_depth != nullptr ? b.grad_depth + static_cast<size_t>(iy) * b.width : nullptr;
+    const unsigned long long key_k = (static_cast<unsigned long long>(q.key_hi) << 32) | q.key_lo;
+    const size_t pix0 = static_cast<size_t>(y) * b.cam.width_int + xs;
+    uint32_t ix = xs / b.ss, sub = xs - ix * b.ss;
+    float fx = static_cast<float>(xs);
+    for (uint32_t i = 0; i < steps; ++i) {
+        if (i < len) {
+            const float dx = fx - q.mx;
+            const float e = dx * (q.cx * dx + cydy) + czdy * dy;
+            const float alpha = q.opacity * exp2f(fminf(e, 0.0f));
+            if (alpha >= kMinAlpha) {
+                const float g0 = g_row[3 * ix + 0] * gs, g1 = g_row[3 * ix + 1] * gs, g2 = g_row[3 * ix + 2] * gs;
+                const float ga = ga_row != nullptr ? ga_row[ix] * gs : 0.0f;
+                const float gd = gd_row != nullptr ? gd_row[ix] * gs : 0.0f;
+                const unsigned long long* keys = b.pix_keys + (pix0 + i) * S;
+                const float* terms = b.pix_terms + (pix0 + i) * S;
+                uint32_t ge = 0, won = 0, none = 0;
+                float behind = 0.0f;
+                uint32_t s = 0;
+                if ((S & 1u) == 0) {
+                    for (; s < S; s += 2) {
+                        const ulonglong2 kk = *reinterpret_cast<const ulonglong2*>(keys + s);
+                        const float2 tt = *reinterpret_cast<const float2*>(terms + s);
+                        ge += (kk.x >= key_k) + (kk.y >= key_k);
+                        won += (kk.x == key_k) + (kk.y == key_k);
+                        none += (kk.x == kEmptyFragment) + (kk.y == kEmptyFragment);
+                        behind += (kk.x > key_k ? tt.x : 0.0f) + (kk.y > key_k ? tt.y : 0.0f);
+                    }
+                }
+                for (; s < S; ++s) {
+                    const unsigned long long kk = keys[s];
+                    ge += kk >= key_k;
+                    won += kk == key_k;
+                    none += kk == kEmptyFragment;
+                    if (kk > key_k) behind += terms[s];
+                }
+                const float inv = 1.0f / fmaxf(1.0f - alpha, 1e-12f);
+                const float gck = g0 * q.ckx + g1 * q.cky + g2 * q.ckz + gd * q.depth;
+                const float dA = static_cast<float>(ge) * gck - inv * behind + inv * ga * static_cast<float>(none);
+                if (won != 0) {
+                    const float wf = static_cast<float>(won);
+                    acc.v[6] += gd * wf;
+                    acc.v[7] += g0 * wf;
+                    acc.v[8] += g1 * wf;
+                    acc.v[9] += g2 * wf;
+                }
+                // alpha = opacity exp(-0.5 (cX dx^2 + cZ dy^2) - cY dx dy)
+                const float dAe = dA * alpha;
+                acc.v[0] += dA * (alpha / q.opacity);
+                acc.v[1] += dAe * (-0.5f * dx * dx);
+                acc.v[2] += dAe * (-dx * dy);
+                acc.v[3] += dAe * (-0.5f * dy * dy);
+                acc.v[4] += dAe * (q.conic_x * dx + q.conic_y * dy);
+                acc.v[5] += dAe * (q.conic_y * dx + q.conic_z * dy);
+            }
+        }
+        fx += 1.0f;
+        if (++sub == b.ss) {
+            sub = 0;
+            ++ix;
+        }
+    }
+}
+
+// One thread per Gaussian: the rows of a warp's 32 Gaussians are laid end to end, 32 per step, and
+// each lane walks one row; the row sums go to per-Gaussian accumulators in shared memory.
+__global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const BackwardParams b) {
+    __shared__ WalkGaussian s_g[kWarpsPerBlock][32];
+    __shared__ float s_acc[kWarpsPerBlock][32][kAccum];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t wib = threadIdx.x >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t upto_mask = kFullMask >> (31u - lane);
+    const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
+    bool active = idx < b.n;
+    const uint32_t g = active ? idx : b.n - 1;
+#pragma unroll
+    for (int i = 0; i < kAccum; ++i) s_acc[wib][lane][i] = 0.0f;
+    Projected p;
+    if (!project_gaussian(active, g, b.means, b.scales, b.rotations, b.opacities, b.w2c, b.cam, p)) return;
+    const PixelRect rect = pixel_rect(p.bounds, b.cam);
+    const bool has_rows = active && rect.width > 0 && rect.height > 0;
+    const uint32_t gmask = __ballot_sync(kFullMask, has_rows);
+    const uint32_t h = has_rows ? rect.height : 0u;
+    const uint32_t row_incl = warp_inclusive_sum(h, lane);
+    const uint32_t total_rows = __shfl_sync(kFullMask, row_incl, 31);
+    const uint32_t slot = __popc(gmask & lt_mask);
+    if (has_rows) {
+        WalkGaussian q;
+        q.mx = p.mean2d.x - 0.5f;
+        q.my = p.mean2d.y - 0.5f;
+        const float3 ce = conic_for_exp2(p.conic);
+        q.cx = ce.x;
+        q.cy = ce.y;
+        q.cz = ce.z;
+        q.opacity = p.opacity;
+        q.span = span_constants(ce.x, ce.y, ce.z, p.opacity);
+        q.conic_x = p.conic.x;
+        q.conic_y = p.conic.y;
+        q.conic_z = p.conic.z;
+        q.depth = p.depth;
+        q.ckx = b.colors[3 * g + 0];
+        q.cky = b.colors[3 * g + 1];
+        q.ckz = b.colors[3 * g + 2];
+        const unsigned long long key = pack_fragment(p.depth, g);
+        q.key_lo = static_cast<uint32_t>(key);
+        q.key_hi = static_cast<uint32_t>(key >> 32);
+        q.x_min = rect.x_min;
+        q.y_min = rect.y_min;
+        q.w = rect.width;
+        q.row_first = row_incl - h;
+        s_g[wib][slot] = q;
+    }
+    __syncwarp();
+    int prev = -1;
+    for (uint32_t base = 0; base < total_rows; base += 32) {
+        const uint32_t rel = (row_incl - h) - base;
+        const uint32_t bits = __reduce_or_sync(kFullMask, (has_rows && rel < 32u) ? (1u << rel) : 0u);
+        const int owner = prev + __popc(bits & upto_mask);
+        prev += __popc(bits);
+        const uint32_t r = base + lane;
+        const bool valid = r < total_rows;
+        const WalkGaussian q = s_g[wib][valid ? owner : 0];
+        FragAccum acc;
+#pragma unroll
+        for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
+        walk_row_gradients(b, q, valid, q.y_min + (r - q.row_first), acc);
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < kAccum; ++i)
+                if (acc.v[i] != 0.0f) atomicAdd(&s_acc[wib][owner][i], acc.v[i]);
+        }
+    }
+    __syncwarp();
+    if (!has_rows) return;
+    float* out = b.accum + static_cast<size_t>(g) * kAccum;
+#pragma unroll
+    for (int i = 0; i < kAccum; ++i) {
+        const float v = s_acc[wib][slot][i];
+        if (v != 0.0f) out[i] += v;
+    }
 }
 
 // Signed SH basis of eval_sh (gs_utils.h:212-243) and its gradient w.r.t. the direction.
@@ -320,6 +521,18 @@ cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream)
 cudaError_t launch_backward_fragments(const BackwardParams& p, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
     fragments_backward_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_sample_terms(const BackwardParams& p, cudaStream_t stream) {
+    if (p.n_fb == 0) return cudaSuccess;
+    sample_terms_kernel<<<(p.n_fb + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStream_t stream) {
+    if (p.n == 0) return cudaSuccess;
+    fragments_samples_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }
 

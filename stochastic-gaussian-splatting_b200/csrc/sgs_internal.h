@@ -147,11 +147,20 @@ struct BackwardParams {
     float* d_rotations;
     float* d_opacities;
     float* d_sh;
+    // fused form over S samples: per framebuffer pixel and sample, the winner key and
+    // T = grad_scale (g . c_w + g_d z_w), interleaved [pixel][sample]
+    unsigned long long* pix_keys;
+    float* pix_terms;
+    uint32_t n_samples;                      // S
+    uint32_t sample;                         // the sample whose terms sample_terms writes
+    uint32_t n_fb;                           // framebuffer pixels
 };
 
 cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_fragments(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_projection(const BackwardParams& p, cudaStream_t stream);
+cudaError_t launch_backward_sample_terms(const BackwardParams& p, cudaStream_t stream);
+cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStream_t stream);
 
 // Sets the calling thread's sgs_last_error() message (printf format) and returns `status`.
 int record_error(int status, const char* fmt, ...);

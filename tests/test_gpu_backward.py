@@ -76,3 +76,84 @@ def test_backward_rejects_unsupported_modes(cuda_device):
     params = [t.cuda().requires_grad_(True) for t in scene.tensors()]
     with pytest.raises(RuntimeError, match="stochastic transparency"):
         render_samples(*params, _settings(cam, 1)._replace(use_gps=True), n_samples=2)
+
+
+@pytest.mark.parametrize("ss,n_samples", [(1, 6), (3, 5), (2, 16)])
+def test_fused_walk_equals_one_walk_per_sample(ss, n_samples, cuda_device):
+    """sgs_backward_sample_terms + sgs_backward_accumulate_samples (one walk for all samples) give the
+    gradients of sgs_backward_accumulate called once per sample, up to float summation order."""
+    import ctypes
+
+    from StochasticGSCudaBackend import _abi
+    from StochasticGSCudaBackend.autograd import _render_one, _structs
+
+    lib = _abi.load()
+    scene, cam, gi, ga, gd = _problem(ss)
+    settings = _settings(cam, ss)
+    tensors = tuple(t.cuda().contiguous() for t in scene.tensors())
+    g, c, s = _structs(*tensors, settings)
+    grads = [torch.tensor(a, dtype=torch.float32, device="cuda").contiguous() for a in (gi, ga, gd)]
+    gp = [ctypes.c_void_p(t.data_ptr()) for t in grads]
+    e = torch.empty(0)
+    hist, workspaces = (e, e, e, e), []
+    for k in range(n_samples):
+        hist, ws, _ = _render_one(tensors, settings, hist, 0 if k == 0 else 1, 300 + k)
+        workspaces.append(ws)
+    weight = ctypes.c_float(1.0 / n_samples)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    nbytes = lib.sgs_backward_workspace_size(tensors[0].shape[0])
+
+    def finish(bw):
+        outs = [torch.empty_like(t) for t in tensors]
+        assert lib.sgs_backward_finish(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(bw.data_ptr()),
+                                       *(ctypes.c_void_p(t.data_ptr()) for t in outs), stream) == _abi.SGS_OK
+        return [t.cpu().numpy() for t in outs]
+
+    bw_a = torch.empty(nbytes // 4 + 4, device="cuda")
+    for k, ws in enumerate(workspaces):
+        assert lib.sgs_backward_accumulate(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(ws.data_ptr()),
+                                           *gp, weight, int(k == 0), ctypes.c_void_p(bw_a.data_ptr()),
+                                           stream) == _abi.SGS_OK
+    per_sample = finish(bw_a)
+
+    bw_b = torch.empty(nbytes // 4 + 4, device="cuda")
+    scratch = torch.empty(lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s), n_samples),
+                          dtype=torch.uint8, device="cuda")
+    for k, ws in enumerate(workspaces):
+        assert lib.sgs_backward_sample_terms(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
+                                             ctypes.c_void_p(ws.data_ptr()), *gp, weight, k, n_samples,
+                                             ctypes.c_void_p(scratch.data_ptr()), stream) == _abi.SGS_OK
+    assert lib.sgs_backward_accumulate_samples(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), *gp, weight,
+                                               n_samples, 1, ctypes.c_void_p(scratch.data_ptr()),
+                                               ctypes.c_void_p(bw_b.data_ptr()), stream) == _abi.SGS_OK
+    fused = finish(bw_b)
+    for k, a, b in zip(KEYS, per_sample, fused):
+        scale = np.abs(a).max()
+        assert scale > 0, k
+        np.testing.assert_allclose(b, a, rtol=2e-3, atol=2e-5 * scale, err_msg=k)
+
+
+def test_fused_walk_rejects_bad_sample_counts(cuda_device):
+    import ctypes
+
+    from StochasticGSCudaBackend import _abi
+    from StochasticGSCudaBackend.autograd import _structs
+
+    lib = _abi.load()
+    scene, cam, *_ = _problem()
+    settings = _settings(cam, 1)
+    tensors = tuple(t.cuda().contiguous() for t in scene.tensors())
+    g, c, s = _structs(*tensors, settings)
+    assert lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s), 0) == 0
+    assert lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s), 1025) == 0
+    gi = torch.zeros((H, W, 3), device="cuda")
+    scratch = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
+    bw = torch.empty(lib.sgs_backward_workspace_size(tensors[0].shape[0]) // 4 + 4, device="cuda")
+    st = lib.sgs_backward_accumulate_samples(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
+                                             ctypes.c_void_p(gi.data_ptr()), None, None, ctypes.c_float(1.0), 0, 1,
+                                             ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(bw.data_ptr()), None)
+    assert st == _abi.SGS_ERROR_INVALID_ARGUMENT
+    st = lib.sgs_backward_sample_terms(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
+                                       ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(gi.data_ptr()), None, None,
+                                       ctypes.c_float(1.0), 4, 4, ctypes.c_void_p(scratch.data_ptr()), None)
+    assert st == _abi.SGS_ERROR_INVALID_ARGUMENT
