@@ -167,7 +167,8 @@ int sgs_backward_finish(const sgs_gaussians* gaussians, const sgs_camera* camera
  *      the next sample once this call is enqueued;
  *   b. sgs_backward_accumulate_samples: the walk; `first` = 1 clears the accumulators.
  * `scratch` holds sgs_backward_samples_scratch_size(camera, settings, S) bytes (12 bytes per
- * framebuffer pixel and sample), 256-byte aligned; S is at most 1024. Same estimator, supported
+ * framebuffer pixel and sample, plus 8 per pixel), 256-byte aligned; S is at most 1024. The samples'
+ * terms must be written in order s = 0, 1, ..., S - 1. Same estimator, supported
  * settings and sgs_backward_finish as above. */
 size_t sgs_backward_samples_scratch_size(const sgs_camera* camera, const sgs_settings* settings, uint32_t n_samples);
 int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,

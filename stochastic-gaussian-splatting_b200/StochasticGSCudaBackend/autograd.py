@@ -10,7 +10,7 @@ csrc/backward_st.cu): each sample's winners give a one-sample estimate, averaged
 Winners are either kept from the forward pass (`store_winners=True`, 24 bytes per framebuffer pixel
 and sample) or recomputed by rendering the same frame indices again (`store_winners=False`: one more
 render per sample, no render workspace kept per sample). Either way the backward first tabulates
-every sample's winner and colour term (12 bytes per framebuffer pixel and sample) and then walks
+every sample's winner and colour term (12 bytes per framebuffer pixel and sample, 8 more per pixel) and then walks
 the Gaussians' fragments once for all samples (sgs_backward_sample_terms,
 sgs_backward_accumulate_samples).
 """

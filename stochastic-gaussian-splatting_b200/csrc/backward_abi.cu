@@ -67,8 +67,10 @@ size_t align256(const size_t v) { return (v + 255) & ~size_t(255); }
 void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples) {
     p.n_samples = n_samples;
     p.pix_keys = static_cast<unsigned long long*>(scratch);
-    p.pix_terms = reinterpret_cast<float*>(static_cast<char*>(scratch) +
-                                           align256(sizeof(unsigned long long) * p.n_fb * static_cast<size_t>(n_samples)));
+    const size_t keys = align256(sizeof(unsigned long long) * p.n_fb * static_cast<size_t>(n_samples));
+    const size_t terms = align256(sizeof(float) * p.n_fb * static_cast<size_t>(n_samples));
+    p.pix_terms = reinterpret_cast<float*>(static_cast<char*>(scratch) + keys);
+    p.pix_max_key = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + keys + terms);
 }
 
 void set_backward_buffers(BackwardParams& p, void* backward_workspace) {
@@ -121,7 +123,8 @@ size_t sgs_backward_samples_scratch_size(const sgs_camera* camera, const sgs_set
     if (camera == nullptr || settings == nullptr || n_samples == 0 || n_samples > kMaxFusedSamples) return 0;
     const uint32_t ss = settings->supersampling_factor < 1 ? 1u : static_cast<uint32_t>(settings->supersampling_factor);
     const size_t n_fb = static_cast<size_t>(camera->width) * ss * camera->height * ss;
-    return align256(sizeof(unsigned long long) * n_fb * n_samples) + align256(sizeof(float) * n_fb * n_samples);
+    return align256(sizeof(unsigned long long) * n_fb * n_samples) + align256(sizeof(float) * n_fb * n_samples) +
+           align256(sizeof(unsigned long long) * n_fb);
 }
 
 int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,

@@ -152,6 +152,9 @@ __global__ void __launch_bounds__(kBlock) fragments_backward_kernel(const Backwa
 // geometric factors once and sums the S samples' contributions:
 //   dL/da_k = ge (g . c_k + g_d z_k) - sum_{key_w > key_k} T / (1 - a_k) + g_a n_none / (1 - a_k)
 // with ge = #samples whose winner is not in front of k and n_none = #samples with no winner.
+// A fragment behind every sample's winner (key_k > the pixel's largest winner key, an empty pixel
+// counting as the largest key) contributes exactly zero; the walk tests that first, so the per-sample
+// table is read only for the fragments in front of some winner.
 
 __global__ void __launch_bounds__(kBlock) sample_terms_kernel(const BackwardParams b) {
     const uint32_t pix = blockIdx.x * kBlock + threadIdx.x;
@@ -165,6 +168,8 @@ __global__ void __launch_bounds__(kBlock) sample_terms_kernel(const BackwardPara
     const size_t slot = static_cast<size_t>(pix) * b.n_samples + b.sample;
     b.pix_keys[slot] = key;
     b.pix_terms[slot] = t * b.grad_scale;
+    // the farthest winner of the samples so far (launches are ordered: sample 0 starts the maximum)
+    b.pix_max_key[pix] = b.sample == 0 ? key : max(b.pix_max_key[pix], key);
 }
 
 // Per-Gaussian constants of the fused walk (96 bytes).
@@ -206,7 +211,7 @@ __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, cons
     uint32_t ix = xs / b.ss, sub = xs - ix * b.ss;
     float fx = static_cast<float>(xs);
     for (uint32_t i = 0; i < steps; ++i) {
-        if (i < len) {
+        if (i < len && key_k <= b.pix_max_key[pix0 + i]) {
             const float dx = fx - q.mx;
             const float e = dx * (q.cx * dx + cydy) + czdy * dy;
             const float alpha = q.opacity * exp2f(fminf(e, 0.0f));

@@ -151,6 +151,7 @@ struct BackwardParams {
     // T = grad_scale (g . c_w + g_d z_w), interleaved [pixel][sample]
     unsigned long long* pix_keys;
     float* pix_terms;
+    unsigned long long* pix_max_key;         // per pixel, the largest winner key of the samples
     uint32_t n_samples;                      // S
     uint32_t sample;                         // the sample whose terms sample_terms writes
     uint32_t n_fb;                           // framebuffer pixels
