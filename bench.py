@@ -452,8 +452,9 @@ def train_measure(dev, views: int = 4, target_spp: int = 64, steps_per_view: int
 
 
 def batch_graph(scene, fl, dev, steps: int) -> dict:
-    """32 views cycling 720p, 1080p, 1440p and 4K on the orbit, one sample each, captured in one CUDA
-    graph (the batched-throughput workload); also the same 32 calls made eagerly."""
+    """32 views cycling 720p, 1080p, 1440p and 4K on the orbit, one sample each, captured in CUDA
+    graphs (the batched-throughput workload; each render split over an accumulate and a resolve
+    stream, histories ping-ponged); also the same step without the graphs."""
     import sgs_batch
 
     res = [(1280, 720), (1920, 1080), (2560, 1440), (3840, 2160)]
@@ -470,13 +471,12 @@ def batch_graph(scene, fl, dev, steps: int) -> dict:
     t1.record(stream)
     torch.cuda.synchronize(dev)
     graph_ms = t0.elapsed_time(t1) / steps
-    hist = [tuple(h) for h in batch.static_out]
     for _ in range(2):
-        hist = batch._render_all(hist, 1)
+        batch.eager_step()
     torch.cuda.synchronize(dev)
     t0.record(stream)
     for _ in range(steps):
-        hist = batch._render_all(hist, 1)
+        batch.eager_step()
     t1.record(stream)
     torch.cuda.synchronize(dev)
     eager_ms = t0.elapsed_time(t1) / steps

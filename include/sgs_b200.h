@@ -123,6 +123,20 @@ int sgs_render(const sgs_gaussians* gaussians, const sgs_camera* camera, const s
                const sgs_history* history, const sgs_outputs* outputs, void* workspace, size_t workspace_bytes,
                void* stream);
 
+/* sgs_render split over two streams (no counterpart in the reference): the framebuffer clear and
+ * the accumulate pass are enqueued on `accumulate_stream`, the sample and resolve passes on
+ * `resolve_stream` behind an event recorded after the accumulate pass. The accumulate pass reads
+ * only the Gaussians, the camera and the workspace, so a following call with another workspace can
+ * accumulate while this one resolves (many views in one CUDA graph, a progressive loop). The caller
+ * orders `accumulate_stream` after its writes of the Gaussians and the camera, and `resolve_stream`
+ * after its writes of the history and k-buffer and before its reads of the outputs; the workspace
+ * must stay untouched until the resolve pass is done. A device-resident frame index is advanced on
+ * `accumulate_stream`. The first call on a host thread creates the event between the streams: make
+ * it before any stream capture. With both streams equal this is sgs_render. */
+int sgs_render_split(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                     const sgs_history* history, const sgs_outputs* outputs, void* workspace, size_t workspace_bytes,
+                     void* accumulate_stream, void* resolve_stream);
+
 /* sgs_render for callers that cannot allocate device memory while rendering (a plugin inside a
  * host application under a fixed memory budget, a C caller without a caching allocator). It has no
  * counterpart in the reference. The caller passes inputs, history and outputs as for sgs_render;

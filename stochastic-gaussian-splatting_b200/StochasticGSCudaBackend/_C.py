@@ -169,7 +169,7 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
     return device, g, c, s, h, (width, height), keep
 
 
-def _render_impl(args, want_workspace: bool):
+def _render_impl(args, want_workspace: bool, streams=None):
     device, g, c, s, h, (width, height), keep = _prepare(*args)
     with torch.cuda.device(device):
         opts = dict(dtype=torch.float32, device=device)
@@ -182,10 +182,26 @@ def _render_impl(args, want_workspace: bool):
         if ws_bytes == 0:
             raise RuntimeError(_abi.last_error(_lib) or "invalid render arguments")
         workspace = torch.empty((ws_bytes,), dtype=torch.uint8, device=device)
-        stream = torch.cuda.current_stream(device).cuda_stream
-        status = _lib.sgs_render(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h), ctypes.byref(o),
-                                 ctypes.c_void_p(workspace.data_ptr()), ctypes.c_size_t(ws_bytes),
-                                 ctypes.c_void_p(stream))
+        if streams is None:
+            stream = torch.cuda.current_stream(device).cuda_stream
+            status = _lib.sgs_render(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h),
+                                     ctypes.byref(o), ctypes.c_void_p(workspace.data_ptr()), ctypes.c_size_t(ws_bytes),
+                                     ctypes.c_void_p(stream))
+        else:
+            acc, res = streams
+            status = _lib.sgs_render_split(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h),
+                                           ctypes.byref(o), ctypes.c_void_p(workspace.data_ptr()),
+                                           ctypes.c_size_t(ws_bytes), ctypes.c_void_p(acc.cuda_stream),
+                                           ctypes.c_void_p(res.cuda_stream))
+            # the caching allocator must not hand these blocks out again before the streams are done
+            for t in (image, depth, alpha, weight_mass):
+                t.record_stream(res)
+            workspace.record_stream(acc)
+            workspace.record_stream(res)
+            for t in keep:
+                if t is not None:
+                    t.record_stream(acc)
+                    t.record_stream(res)
         if status != _abi.SGS_OK:
             raise RuntimeError(f"sgs_render failed ({status}): {_abi.last_error(_lib)}")
         del keep
@@ -201,6 +217,57 @@ def render(*args):
     if len(args) != 29:
         raise TypeError(f"render() takes 29 positional arguments ({len(args)} given)")
     return _render_impl(args, want_workspace=False)
+
+
+def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cuda.Stream, *args):
+    """As `render` (the same 29 arguments after the two streams), with the clear and accumulate passes
+    enqueued on `accumulate_stream` and the sample and resolve passes on `resolve_stream` (the C ABI's
+    sgs_render_split): a following call can accumulate while this one resolves. The outputs are
+    complete on `resolve_stream`; the caller orders its other streams against the two."""
+    if len(args) != 29:
+        raise TypeError(f"render_split() takes 2 streams and 29 positional arguments ({len(args)} given)")
+    return _render_impl(args, want_workspace=False, streams=(accumulate_stream, resolve_stream))
+
+
+def workspace_size(*args) -> int:
+    """Bytes of scratch a render with these 29 `render` arguments needs (sgs_workspace_size)."""
+    _, g, c, s, _, _, _ = _prepare(*args)
+    n = int(_lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s)))
+    if n == 0:
+        raise RuntimeError(_abi.last_error(_lib) or "invalid render arguments")
+    return n
+
+
+def render_into(outputs, workspace: torch.Tensor, streams, *args) -> None:
+    """Renders like `render` into caller-owned buffers: `outputs` = (image (H, W, 3), depth, alpha,
+    weight_mass (H, W, 1)) float32 CUDA tensors, `workspace` a uint8 CUDA tensor of at least
+    `workspace_size(*args)` bytes (256-byte aligned), `streams` = None (current stream) or
+    (accumulate stream, resolve stream) as in `render_split`. Nothing is allocated, so the call can
+    be captured in a CUDA graph with fixed buffers (for example ping-ponged histories)."""
+    if len(args) != 29:
+        raise TypeError(f"render_into() takes outputs, workspace, streams and 29 render arguments ({len(args)} given)")
+    device, g, c, s, h, (width, height), keep = _prepare(*args)
+    shapes = ((height, width, 3), (height, width, 1), (height, width, 1), (height, width, 1))
+    for name, t, shape in zip(("image", "depth", "alpha", "weight_mass"), outputs, shapes):
+        _check(isinstance(t, torch.Tensor) and t.is_cuda and t.device == device and t.dtype == torch.float32
+               and tuple(t.shape) == shape and t.is_contiguous(),
+               f"output {name} must be a contiguous {shape} float32 CUDA tensor on {device}")
+    ws_bytes = int(_lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s)))
+    _check(ws_bytes > 0, _abi.last_error(_lib) or "invalid render arguments")
+    _check(workspace.is_cuda and workspace.device == device and workspace.dtype == torch.uint8
+           and workspace.numel() >= ws_bytes and workspace.data_ptr() % 256 == 0,
+           f"workspace must be a 256-byte aligned uint8 CUDA tensor of at least {ws_bytes} bytes")
+    o = _abi.Outputs(*(t.data_ptr() for t in outputs))
+    if streams is None:
+        acc = res = torch.cuda.current_stream(device)
+    else:
+        acc, res = streams
+    status = _lib.sgs_render_split(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h), ctypes.byref(o),
+                                   ctypes.c_void_p(workspace.data_ptr()), ctypes.c_size_t(workspace.numel()),
+                                   ctypes.c_void_p(acc.cuda_stream), ctypes.c_void_p(res.cuda_stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_render_split failed ({status}): {_abi.last_error(_lib)}")
+    del keep
 
 
 def render_with_workspace(*args):

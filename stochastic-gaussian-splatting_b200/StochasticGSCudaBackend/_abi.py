@@ -119,6 +119,9 @@ SIGNATURES = {
     "sgs_render": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC),
                                   ctypes.POINTER(HistoryC), ctypes.POINTER(Outputs), ctypes.c_void_p, ctypes.c_size_t,
                                   ctypes.c_void_p]),
+    "sgs_render_split": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC),
+                                        ctypes.POINTER(HistoryC), ctypes.POINTER(Outputs), ctypes.c_void_p,
+                                        ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_render_no_alloc": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
                                            ctypes.POINTER(SettingsC), ctypes.POINTER(HistoryC),
                                            ctypes.POINTER(Outputs), ctypes.c_void_p]),

@@ -193,8 +193,20 @@ int sgs_get_workspace_layout(const sgs_gaussians* gaussians, const sgs_camera* c
     return SGS_OK;
 }
 
-int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, const sgs_history* h,
-               const sgs_outputs* o, void* workspace, size_t workspace_bytes, void* stream_ptr) {
+}  // extern "C"
+
+namespace {
+
+// Event between the accumulate and the resolve stream of split renders (one per host thread).
+thread_local cudaEvent_t t_split_event = nullptr;
+
+__global__ void advance_frame_kernel(uint32_t* frame_counter) { *frame_counter += 1u; }
+
+// The render of sgs_render / sgs_render_split: clear and accumulate on `acc_stream`, sample and
+// resolve on `res_stream` (the same stream for sgs_render).
+int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, const sgs_history* h,
+                      const sgs_outputs* o, void* workspace, size_t workspace_bytes, cudaStream_t acc_stream,
+                      cudaStream_t res_stream) {
     t_last_error.clear();
     Derived d;
     int st = derive(g, c, s, d);
@@ -227,7 +239,13 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     if (workspace_bytes < L.total)
         return fail(SGS_ERROR_WORKSPACE, "workspace has %zu bytes, needs %zu", workspace_bytes, L.total);
 
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const bool split = acc_stream != res_stream;
+    if (split && t_split_event == nullptr &&
+        cudaEventCreateWithFlags(&t_split_event, cudaEventDisableTiming) != cudaSuccess) {
+        t_split_event = nullptr;
+        return fail(SGS_ERROR_CUDA, "could not create the event between the accumulate and resolve streams");
+    }
+    cudaStream_t stream = acc_stream;
     char* ws = static_cast<char*>(workspace);
     // the host counter serves calls that keep no frame index in device memory
     const uint32_t frame =
@@ -313,9 +331,38 @@ int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* 
     rp.sh_vec4 = g->sh_bases == 16 && aligned16(g->sh_coefficients);
     rp.frame_counter = s->frame_index_device;
     rp.temporal_mode = s->temporal_mode;
-    err = launch_sample_resolve(rp, stream);
+    if (split) {
+        // the next call's accumulate pass may start before this resolve: advance the device-resident
+        // frame index behind this accumulate pass instead
+        if (s->frame_index_device != nullptr) {
+            advance_frame_kernel<<<1, 1, 0, acc_stream>>>(s->frame_index_device);
+            rp.frame_counter = nullptr;
+        }
+        err = cudaEventRecord(t_split_event, acc_stream);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(res_stream, t_split_event, 0);
+        if (err == cudaSuccess) err = cudaGetLastError();
+        if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "stream split: %s", cudaGetErrorString(err));
+    }
+    err = launch_sample_resolve(rp, res_stream);
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));
     return SGS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sgs_render(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, const sgs_history* h,
+               const sgs_outputs* o, void* workspace, size_t workspace_bytes, void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return render_on_streams(g, c, s, h, o, workspace, workspace_bytes, st, st);
+}
+
+int sgs_render_split(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, const sgs_history* h,
+                     const sgs_outputs* o, void* workspace, size_t workspace_bytes, void* accumulate_stream,
+                     void* resolve_stream) {
+    return render_on_streams(g, c, s, h, o, workspace, workspace_bytes, static_cast<cudaStream_t>(accumulate_stream),
+                             static_cast<cudaStream_t>(resolve_stream));
 }
 
 void sgs_set_queue_limit(uint32_t max_entries) { g_queue_limit.store(max_entries, std::memory_order_relaxed); }

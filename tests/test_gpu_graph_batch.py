@@ -80,3 +80,52 @@ def test_device_counter_does_not_touch_the_process_counter(cuda_device):
     _C.set_frame_index(8)
     d = _C.render(*args)
     assert torch.equal(a[0], c[0]) and torch.equal(b[0], d[0]) and not torch.equal(a[0], b[0])
+
+
+@pytest.mark.parametrize("flags", [dict(aa=False, ss=1, gps=False, hybrid=False),
+                                   dict(aa=True, ss=2, gps=False, hybrid=True),
+                                   dict(aa=False, ss=1, gps=True, hybrid=True)])
+def test_split_streams_and_caller_buffers_equal_render(flags, cuda_device):
+    """render_split (accumulate and resolve on two streams) and render_into (caller buffers) give the
+    outputs of render, frame for frame, in Reset and Static mode."""
+    scene = sgs_scenes.make_scene(sgs_scenes.SceneSpec(n=50_000, log_scale_mean=-3.0, log_scale_std=0.8), seed=4)
+    tensors = tuple(t.cuda() for t in scene.tensors())
+    cam = sgs_scenes.front_camera(160, 120)
+    ss = flags["ss"]
+    n_fb = 160 * 120 * ss * ss
+    kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device="cuda"), torch.empty((0, n_fb, 4), device="cuda"))
+    e = torch.empty(0)
+
+    def args(hist, mode):
+        return (*tensors, cam.w2c.cuda(), cam.position.cuda(), 160, 120, cam.focal_x, cam.focal_y, cam.center_x,
+                cam.center_y, cam.near_plane, cam.far_plane, flags["aa"], ss, flags["gps"], flags["hybrid"], False,
+                torch.empty(0, dtype=torch.uint8, device="cuda"), *kb, *hist, torch.eye(4, device="cuda"), mode)
+
+    acc, res = torch.cuda.Stream(), torch.cuda.Stream()
+    cur = torch.cuda.current_stream()
+    h_ref = h_split = h_into = (e, e, e, e)
+    outs = tuple(torch.empty((120, 160, ch), device="cuda") for ch in (3, 1, 1, 1))
+    outs2 = tuple(torch.empty_like(t) for t in outs)
+    ws = torch.empty(_C.workspace_size(*args((e, e, e, e), 0)), dtype=torch.uint8, device="cuda")
+    for k in range(3):
+        mode = 0 if k == 0 else 1
+        _C.set_frame_index(40 + k)
+        h_ref = _C.render(*args(h_ref, mode))
+        _C.set_frame_index(40 + k)
+        acc.wait_stream(cur)
+        res.wait_stream(cur)
+        h_split = _C.render_split(acc, res, *args(h_split, mode))
+        cur.wait_stream(res)
+        _C.set_frame_index(40 + k)
+        dst = outs if k % 2 == 0 else outs2
+        acc.wait_stream(cur)
+        res.wait_stream(cur)
+        _C.render_into(dst, ws, (acc, res), *args(h_into, mode))
+        cur.wait_stream(res)
+        cur.wait_stream(acc)
+        h_into = dst
+        for name, a, b, c in zip(("image", "depth", "alpha", "weight_mass"), h_ref, h_split, h_into):
+            assert torch.equal(a, b), f"render_split, frame {k}, {name}"
+            assert torch.equal(a, c), f"render_into, frame {k}, {name}"
+    with pytest.raises(RuntimeError, match="workspace"):
+        _C.render_into(outs, ws[:64], None, *args((e, e, e, e), 0))
