@@ -7,9 +7,10 @@
 // pixel) and the merge is a minimum, so the result does not depend on which thread evaluates
 // which fragment. This file uses that freedom for a B200-oriented schedule:
 //
-//  * rows, then spans: a warp expands its 32 Gaussians into AABB rows, 32 rows at a time, and each
-//    lane computes the conservative x-span of the alpha >= 1/255 ellipse on its row (the AABB
-//    corners, ~45% of its pixels, are never evaluated);
+//  * rows, then spans: a warp sorts its 32 Gaussians by their widest span (a bitonic network over
+//    the lanes), expands them into AABB rows in that order, 32 rows at a time, and each lane
+//    computes the conservative x-span of the alpha >= 1/255 ellipse on its row (the AABB corners,
+//    ~45% of its pixels, are never evaluated);
 //  * each lane then walks its own row two pixels per step, the alpha exponent of both pixels in
 //    packed FP32x2 instructions (fma/mul/sub .f32x2 of sm_100a, each element rounded like the scalar
 //    instruction), with no per-pixel owner lookup or shared-memory traffic; the warp steps as often
@@ -130,6 +131,23 @@ __device__ __forceinline__ uint32_t row_seed(const FrameRng& rng, const uint32_t
     return key_lo ^ (rng.frame * 1973u) ^ (y * 2699u);
 }
 
+// Sorting key of Gaussians without rows (they go after every Gaussian with rows).
+constexpr uint32_t kNoRowsKey = (1u << 26) - 1u;
+
+// Bitonic sort of one 32-bit value per lane, ascending over the lanes (values distinct).
+__device__ __forceinline__ uint32_t warp_sort_ascending(uint32_t v, const uint32_t lane) {
+#pragma unroll
+    for (uint32_t k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t other = __shfl_xor_sync(kFullMask, v, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = keep_min ? min(v, other) : max(v, other);
+        }
+    }
+    return v;
+}
+
 // One predicated 64-bit RED.MIN (no branch around it).
 __device__ __forceinline__ void red_min_if(unsigned long long* address, const unsigned long long key, const bool pred) {
     asm volatile(
@@ -217,6 +235,7 @@ __device__ __forceinline__ void walk_chunk(const AccumulateParams& a, const Fram
 template <bool kBlue, bool kHybrid>
 __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateParams a) {
     __shared__ RowGaussian s_gauss[kWarpsPerBlock][32];
+    __shared__ uint32_t s_rank[kWarpsPerBlock][32];
 
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t wib = threadIdx.x >> 5;
@@ -284,16 +303,32 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         }
     }
 
-    // level 1: the rows of this warp's Gaussians, end to end
-    const uint32_t gmask = __ballot_sync(kFullMask, has_rows);
+    // level 1: the rows of this warp's Gaussians, end to end, the Gaussians ordered by their widest
+    // span so that the 32 rows walked together have similar lengths (a warp walks as long as its
+    // longest row); Gaussians without rows go last
+    uint32_t width_key = kNoRowsKey;
+    if (has_rows) {
+        uint32_t widest = G.w;
+        if (G.span.k2 > 0.0f) {
+            const float est = 2.0f * sqrtf(G.span.k2 * G.span.dymax2) + 2.0f;
+            if (est < static_cast<float>(widest)) widest = static_cast<uint32_t>(est);
+        }
+        width_key = min(widest, kNoRowsKey - 1u);
+    }
+    const uint32_t sorted = warp_sort_ascending((width_key << 5) | lane, lane);  // lane i: i-th smallest
+    const uint32_t src_lane = sorted & 31u;
+    s_rank[wib][src_lane] = lane;
     const uint32_t h = has_rows ? rect.height : 0u;
-    const uint32_t row_incl = warp_inclusive_sum(h, lane);
-    const uint32_t total_rows = __shfl_sync(kFullMask, row_incl, 31);
-    const uint32_t row_first = row_incl - h;
+    const uint32_t h_sorted = __shfl_sync(kFullMask, h, src_lane);
+    const uint32_t incl_sorted = warp_inclusive_sum(h_sorted, lane);
+    const uint32_t total_rows = __shfl_sync(kFullMask, incl_sorted, 31);
+    __syncwarp();
+    const uint32_t rank = s_rank[wib][lane];
+    const uint32_t row_first = __shfl_sync(kFullMask, incl_sorted - h_sorted, rank);
     if (has_rows) {
         RowGaussian st = G;
         st.row_first = row_first;
-        s_gauss[wib][__popc(gmask & lt_mask)] = st;
+        s_gauss[wib][rank] = st;
     }
     __syncwarp();
     int prev = -1;
