@@ -73,20 +73,46 @@ void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples
     p.pix_max_key = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + keys + terms);
 }
 
+// Entries of the large-Gaussian queue of the fused walk (at most 2^18).
+uint32_t queue_capacity(const uint32_t n) { return n < (1u << 18) ? n : (1u << 18); }
+constexpr size_t kWalkGaussianBytes = 96;
+
+// Backward workspace: colours (3 per Gaussian, padded to 4), accumulators (10 per Gaussian), then
+// the fused walk's queue (header, entries, meta, indices), each section 256-byte aligned.
+struct BackwardLayout {
+    size_t colors, accum, queue, entries, meta, index, total;
+};
+
+BackwardLayout backward_layout(const uint32_t n) {
+    BackwardLayout L{};
+    const size_t cap = queue_capacity(n);
+    L.colors = 0;
+    L.accum = align256(sizeof(float) * ((3 * static_cast<size_t>(n) + 3) & ~size_t(3)));
+    L.queue = L.accum + align256(sizeof(float) * kAccumFloats * n);
+    L.entries = L.queue + align256(sizeof(WorkQueue));
+    L.meta = L.entries + align256(kWalkGaussianBytes * cap);
+    L.index = L.meta + align256(sizeof(uint4) * cap);
+    L.total = L.index + align256(sizeof(uint32_t) * cap);
+    return L;
+}
+
 void set_backward_buffers(BackwardParams& p, void* backward_workspace) {
-    float* base = static_cast<float*>(backward_workspace);
-    p.colors = base;
-    p.accum = base + ((3 * static_cast<size_t>(p.n) + 3) & ~size_t(3));
+    char* base = static_cast<char*>(backward_workspace);
+    const BackwardLayout L = backward_layout(p.n);
+    p.colors = reinterpret_cast<float*>(base + L.colors);
+    p.accum = reinterpret_cast<float*>(base + L.accum);
+    p.bw_queue = reinterpret_cast<WorkQueue*>(base + L.queue);
+    p.bw_entries = base + L.entries;
+    p.bw_meta = reinterpret_cast<uint4*>(base + L.meta);
+    p.bw_index = reinterpret_cast<uint32_t*>(base + L.index);
+    p.bw_capacity = queue_capacity(p.n);
 }
 
 }  // namespace
 
 extern "C" {
 
-size_t sgs_backward_workspace_size(uint32_t n_gaussians) {
-    const size_t colors = (3 * static_cast<size_t>(n_gaussians) + 3) & ~size_t(3);
-    return (colors + kAccumFloats * n_gaussians) * sizeof(float);
-}
+size_t sgs_backward_workspace_size(uint32_t n_gaussians) { return backward_layout(n_gaussians).total; }
 
 int sgs_backward_accumulate(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
                             const void* render_workspace, const float* grad_image, const float* grad_alpha,
@@ -181,6 +207,12 @@ int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_ca
     if (first) {
         err = cudaMemsetAsync(p.accum, 0, kAccumFloats * p.n * sizeof(float), stream);
         if (err == cudaSuccess) err = launch_backward_colors(p, stream);
+    }
+    if (err == cudaSuccess) err = cudaMemsetAsync(p.bw_queue, 0, sizeof(WorkQueue), stream);
+    if (err == cudaSuccess) {
+        int device = 0;
+        err = cudaGetDevice(&device);
+        if (err == cudaSuccess) err = cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, device);
     }
     if (err == cudaSuccess) err = launch_backward_fragments_samples(p, stream);
     if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));

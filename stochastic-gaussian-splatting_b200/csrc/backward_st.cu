@@ -27,6 +27,9 @@ constexpr uint32_t kBlock = 256;
 constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kFullMask = 0xffffffffu;
 constexpr uint32_t kCoopFragments = 64;  // larger AABBs are processed by the whole warp
+constexpr uint32_t kBigFragments = 2048;  // fused walk: larger AABBs go to the row-chunk queue
+constexpr uint32_t kChunkPixels = 2048;   // pixels per stolen chunk (whole rows, at most 32)
+constexpr uint32_t kQueueBlocksPerSM = 8;
 constexpr int kAccum = 10;               // op, conic x/y/z, mean2d x/y, depth, colour r/g/b
 
 // View-dependent colour of every Gaussian (the colour its fragments would give a pixel).
@@ -172,6 +175,13 @@ __global__ void __launch_bounds__(kBlock) sample_terms_kernel(const BackwardPara
     b.pix_max_key[pix] = b.sample == 0 ? key : max(b.pix_max_key[pix], key);
 }
 
+// Rows per chunk of a queued Gaussian of AABB width w (log2): about kChunkPixels pixels, a power of
+// two between 1 and 32; each row of a chunk is walked in 32 / rows segments.
+__device__ __forceinline__ uint32_t log_chunk_rows(const uint32_t w) {
+    const uint32_t rows = max(1u, min(32u, kChunkPixels / max(w, 1u)));
+    return 31u - __clz(rows);
+}
+
 // Per-Gaussian constants of the fused walk (96 bytes).
 struct WalkGaussian {
     float mx, my;             // mean2d - 0.5
@@ -186,16 +196,25 @@ struct WalkGaussian {
     uint32_t row_first;       // first row position in the warp's row list
     uint32_t pad[2];
 };
+static_assert(sizeof(WalkGaussian) == 96, "the backward workspace reserves 96 bytes per queue entry");
+
 
 // Lane walks the span of row y of Gaussian q (when valid), one pixel per step, and adds the S
 // samples' fragment gradients to acc.
 __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, const WalkGaussian& q, const bool valid,
-                                                   const uint32_t y, FragAccum& acc) {
+                                                   const uint32_t y, FragAccum& acc, const uint32_t seg = 0,
+                                                   const uint32_t log_segs = 0) {
     uint32_t xs = 0, len = 0;
     float dy = 0.0f;
     if (valid) {
         dy = static_cast<float>(y) - q.my;
         row_span(q.x_min, q.w, q.mx, q.span, dy, xs, len);
+        if (log_segs > 0) {
+            const uint32_t part = (len + (1u << log_segs) - 1u) >> log_segs;
+            const uint32_t skip = min(seg * part, len);
+            xs += skip;
+            len = min(len - skip, part);
+        }
     }
     const uint32_t steps = __reduce_max_sync(kFullMask, len);
     if (steps == 0) return;
@@ -286,14 +305,9 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
     Projected p;
     if (!project_gaussian(active, g, b.means, b.scales, b.rotations, b.opacities, b.w2c, b.cam, p)) return;
     const PixelRect rect = pixel_rect(p.bounds, b.cam);
-    const bool has_rows = active && rect.width > 0 && rect.height > 0;
-    const uint32_t gmask = __ballot_sync(kFullMask, has_rows);
-    const uint32_t h = has_rows ? rect.height : 0u;
-    const uint32_t row_incl = warp_inclusive_sum(h, lane);
-    const uint32_t total_rows = __shfl_sync(kFullMask, row_incl, 31);
-    const uint32_t slot = __popc(gmask & lt_mask);
+    bool has_rows = active && rect.width > 0 && rect.height > 0;
+    WalkGaussian q;
     if (has_rows) {
-        WalkGaussian q;
         q.mx = p.mean2d.x - 0.5f;
         q.my = p.mean2d.y - 0.5f;
         const float3 ce = conic_for_exp2(p.conic);
@@ -315,6 +329,28 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
         q.x_min = rect.x_min;
         q.y_min = rect.y_min;
         q.w = rect.width;
+        q.row_first = 0;
+        // large footprints go to the queue (walked in row chunks across all SMs) unless it is full
+        if (rect.width * rect.height > kBigFragments) {
+            const uint32_t log_rpc = log_chunk_rows(rect.width);
+            const uint32_t chunks = (rect.height + (1u << log_rpc) - 1u) >> log_rpc;
+            const unsigned long long old = atomicAdd(&b.bw_queue->packed, (1ull << kQueueEntryShift) | chunks);
+            const uint32_t e = static_cast<uint32_t>(old >> kQueueEntryShift);
+            const unsigned long long first_chunk = old & kQueueChunkMask;
+            if (e < b.bw_capacity && first_chunk + chunks <= 0xffffffffull) {
+                static_cast<WalkGaussian*>(b.bw_entries)[e] = q;
+                b.bw_meta[e] = make_uint4(rect.y_min, rect.height, log_rpc, static_cast<uint32_t>(first_chunk));
+                b.bw_index[e] = g;
+                has_rows = false;
+            }
+        }
+    }
+    const uint32_t gmask = __ballot_sync(kFullMask, has_rows);
+    const uint32_t h = has_rows ? rect.height : 0u;
+    const uint32_t row_incl = warp_inclusive_sum(h, lane);
+    const uint32_t total_rows = __shfl_sync(kFullMask, row_incl, 31);
+    const uint32_t slot = __popc(gmask & lt_mask);
+    if (has_rows) {
         q.row_first = row_incl - h;
         s_g[wib][slot] = q;
     }
@@ -327,11 +363,11 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
         prev += __popc(bits);
         const uint32_t r = base + lane;
         const bool valid = r < total_rows;
-        const WalkGaussian q = s_g[wib][valid ? owner : 0];
+        const WalkGaussian rq = s_g[wib][valid ? owner : 0];
         FragAccum acc;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
-        walk_row_gradients(b, q, valid, q.y_min + (r - q.row_first), acc);
+        walk_row_gradients(b, rq, valid, rq.y_min + (r - rq.row_first), acc);
         if (valid) {
 #pragma unroll
             for (int i = 0; i < kAccum; ++i)
@@ -345,6 +381,53 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
     for (int i = 0; i < kAccum; ++i) {
         const float v = s_acc[wib][slot][i];
         if (v != 0.0f) out[i] += v;
+    }
+}
+
+// Persistent consumer of the fused walk's large-Gaussian queue: each warp steals one chunk of rows
+// (R rows, each split into 32 / R lane segments), sums the lanes' gradients and adds them to the
+// Gaussian's accumulators.
+__global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const BackwardParams b) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned long long packed = b.bw_queue->packed;
+    const uint32_t n_entries =
+        static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(b.bw_capacity)));
+    if (n_entries == 0) return;
+    const uint4 last = b.bw_meta[n_entries - 1];
+    const uint32_t n_chunks = last.w + ((last.y + (1u << last.z) - 1u) >> last.z);
+    const WalkGaussian* entries = static_cast<const WalkGaussian*>(b.bw_entries);
+    for (;;) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(&b.bw_queue->next_chunk, 1u);
+        c = __shfl_sync(kFullMask, c, 0);
+        if (c >= n_chunks) break;
+        uint32_t lo = 0, hi = n_entries - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (b.bw_meta[mid].w <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const uint4 m = b.bw_meta[lo];
+        const uint32_t log_rows = m.z;
+        const uint32_t r0 = (c - m.w) << log_rows;
+        if (r0 >= m.y || log_rows > 5u) {
+            if (lane == 0) atomicOr(&b.bw_queue->error, 1u);
+            continue;
+        }
+        const WalkGaussian q = entries[lo];
+        const uint32_t r = r0 + (lane & ((1u << log_rows) - 1u));
+        FragAccum acc;
+#pragma unroll
+        for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
+        walk_row_gradients(b, q, r < m.y, q.y_min + r, acc, lane >> log_rows, 5u - log_rows);
+        float* out = b.accum + static_cast<size_t>(b.bw_index[lo]) * kAccum;
+#pragma unroll
+        for (int i = 0; i < kAccum; ++i) {
+            float v = acc.v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+            if (lane == 0 && v != 0.0f) atomicAdd(out + i, v);
+        }
     }
 }
 
@@ -538,6 +621,7 @@ cudaError_t launch_backward_sample_terms(const BackwardParams& p, cudaStream_t s
 cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
     fragments_samples_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    fragments_samples_queue_kernel<<<static_cast<unsigned>(max(p.num_sms, 1)) * kQueueBlocksPerSM, kBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }
 

@@ -152,6 +152,13 @@ struct BackwardParams {
     unsigned long long* pix_keys;
     float* pix_terms;
     unsigned long long* pix_max_key;         // per pixel, the largest winner key of the samples
+    // queue of Gaussians with large footprints, walked in row chunks by a persistent kernel
+    WorkQueue* bw_queue;
+    void* bw_entries;                        // WalkGaussian per entry (backward_st.cu)
+    uint4* bw_meta;                          // y_min, height, log2 rows per chunk, first chunk
+    uint32_t* bw_index;                      // Gaussian index per entry
+    uint32_t bw_capacity;
+    int num_sms;
     uint32_t n_samples;                      // S
     uint32_t sample;                         // the sample whose terms sample_terms writes
     uint32_t n_fb;                           // framebuffer pixels

@@ -78,17 +78,33 @@ def test_backward_rejects_unsupported_modes(cuda_device):
         render_samples(*params, _settings(cam, 1)._replace(use_gps=True), n_samples=2)
 
 
-@pytest.mark.parametrize("ss,n_samples", [(1, 6), (3, 5), (2, 16)])
-def test_fused_walk_equals_one_walk_per_sample(ss, n_samples, cuda_device):
-    """sgs_backward_sample_terms + sgs_backward_accumulate_samples (one walk for all samples) give the
-    gradients of sgs_backward_accumulate called once per sample, up to float summation order."""
+def _big_problem(ss=1):
+    """Footprints of several thousand (sub)pixels, wide and narrow: the fused walk queues them and walks
+    their rows in chunks and lane segments."""
+    spec = sgs_scenes.SceneSpec(n=60, log_scale_mean=-1.2, log_scale_std=0.5, opacity_logit_std=1.0)
+    scene = sgs_scenes.make_scene(spec, seed=8, morton=False)
+    g = torch.Generator().manual_seed(9)
+    scales = scene.scales.clone()
+    scales[:20, 1] -= 2.5  # flat, wide footprints
+    scene = sgs_scenes.Scene(scene.means, scales, scene.rotations, scene.opacities, scene.sh_coefficients)
+    cam = sgs_scenes.pinhole((0.3, -0.2, -4.0), W, H, 60.0)
+    rng = np.random.default_rng(1)
+    return scene, cam, rng.normal(size=(H, W, 3)), rng.normal(size=(H, W, 1)), rng.normal(size=(H, W, 1)) * 0.1
+
+
+@pytest.mark.parametrize("ss,n_samples,big", [(1, 6, False), (3, 5, False), (2, 16, False), (2, 7, True),
+                                              (3, 4, True)])
+def test_fused_walk_equals_one_walk_per_sample(ss, n_samples, big, cuda_device):
+    """sgs_backward_sample_terms + sgs_backward_accumulate_samples (one walk for all samples, large
+    footprints through the row-chunk queue) give the gradients of sgs_backward_accumulate called once
+    per sample, up to float summation order."""
     import ctypes
 
     from StochasticGSCudaBackend import _abi
     from StochasticGSCudaBackend.autograd import _render_one, _structs
 
     lib = _abi.load()
-    scene, cam, gi, ga, gd = _problem(ss)
+    scene, cam, gi, ga, gd = _big_problem(ss) if big else _problem(ss)
     settings = _settings(cam, ss)
     tensors = tuple(t.cuda().contiguous() for t in scene.tensors())
     g, c, s = _structs(*tensors, settings)
