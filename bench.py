@@ -361,6 +361,8 @@ def run_ours(args, world, rank, local) -> dict | None:
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clock_info,
     }
+    if not fl["gps"]:
+        line["samples_per_call"] = samples_per_call(scene, cam, fl, dev, n_samples=8, calls=max(4, args.steps // 8))
     if not args.no_batch and args.workload.startswith("batch_6m"):
         line["batch32_graph"] = batch_graph(scene, fl, dev, steps=max(4, args.steps // 8))
     if not (args.no_train and args.no_learned) and args.workload.startswith("batch_6m"):
@@ -449,6 +451,35 @@ def train_measure(dev, views: int = 4, target_spp: int = 64, steps_per_view: int
             "ms_per_step": round(ms, 3), "steps_per_s": round(1000.0 / ms, 2),
             "loss_first_epoch": round(sum(losses) / len(losses), 5),
             "loss_last_epoch": round(float(sum(last[-views:]) / views), 5)}
+
+
+def samples_per_call(scene, cam, fl, dev, n_samples: int, calls: int) -> dict:
+    """The same workload with `n_samples` samples per call (`_C.render_samples`: one fragment walk and
+    one resolve pass for all of them, outputs equal to one call per sample), Static mode."""
+    from StochasticGSCudaBackend import _C
+
+    W, H, ss = cam.width, cam.height, fl["ss"]
+    n_fb = W * H * ss * ss
+    kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device=dev), torch.empty((0, n_fb, 4), device=dev))
+    e = torch.empty(0)
+    args = lambda hist, mode: (*scene.tensors(), cam.w2c.to(dev), cam.position.to(dev), W, H, cam.focal_x,
+                               cam.focal_y, cam.center_x, cam.center_y, cam.near_plane, cam.far_plane, fl["aa"], ss,
+                               fl["gps"], fl["hybrid"], False, torch.empty(0, dtype=torch.uint8, device=dev), *kb,
+                               *hist, torch.eye(4, device=dev), mode)
+    hist = _C.render_samples(n_samples, *args((e, e, e, e), 0))
+    for _ in range(2):
+        hist = _C.render_samples(n_samples, *args(hist, 1))
+    stream = torch.cuda.current_stream(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    t0.record(stream)
+    for _ in range(calls):
+        hist = _C.render_samples(n_samples, *args(hist, 1))
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = t0.elapsed_time(t1) / (calls * n_samples)
+    return {"samples_per_call": n_samples, "ms_per_sample": round(ms, 5),
+            "sample_frames_per_s": round(1000.0 / ms, 1)}
 
 
 def batch_graph(scene, fl, dev, steps: int) -> dict:

@@ -137,6 +137,21 @@ int sgs_render_split(const sgs_gaussians* gaussians, const sgs_camera* camera, c
                      const sgs_history* history, const sgs_outputs* outputs, void* workspace, size_t workspace_bytes,
                      void* accumulate_stream, void* resolve_stream);
 
+/* Several samples in one call (no counterpart in the reference; it is the sample loop of
+ * Renderer.py:85-87 moved onto the device): renders n_samples samples with frame indices f .. f + n - 1
+ * (f = the current frame index, which advances by n) and merges them into the history in order, the
+ * first in settings->temporal_mode (Reset or Static) and the rest Static. The outputs equal those of
+ * n_samples sgs_render calls bit for bit. One walk over the Gaussians' fragments evaluates each
+ * fragment's alpha once and every sample's threshold, and one resolve pass reads the history once.
+ * Stochastic transparency only, without spatial reuse or Reproject (SGS_ERROR_INVALID_ARGUMENT);
+ * n_samples from 1 to 1024. The workspace holds sgs_samples_workspace_size(..., n_samples) bytes
+ * (n_samples framebuffers). */
+size_t sgs_samples_workspace_size(const sgs_gaussians* gaussians, const sgs_camera* camera,
+                                  const sgs_settings* settings, uint32_t n_samples);
+int sgs_render_samples(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
+                       const sgs_history* history, const sgs_outputs* outputs, uint32_t n_samples, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
 /* sgs_render for callers that cannot allocate device memory while rendering (a plugin inside a
  * host application under a fixed memory budget, a C caller without a caching allocator). It has no
  * counterpart in the reference. The caller passes inputs, history and outputs as for sgs_render;

@@ -229,6 +229,44 @@ def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cud
     return _render_impl(args, want_workspace=False, streams=(accumulate_stream, resolve_stream))
 
 
+def render_samples(n_samples: int, *args):
+    """`n_samples` samples in one call (the C ABI's sgs_render_samples): the same 29 arguments as
+    `render`, frames f .. f + n_samples - 1 merged in order (the first in the given temporal mode,
+    Reset or Static, the rest Static); returns the final (image, depth, alpha, weight_mass), equal
+    bit for bit to `n_samples` `render` calls. Stochastic transparency without spatial reuse."""
+    if len(args) != 29:
+        raise TypeError(f"render_samples() takes n_samples and 29 render arguments ({len(args)} given)")
+    n = int(n_samples)
+    _check(1 <= n <= 1024, f"n_samples must be between 1 and 1024, got {n}")
+    device = args[0].device if isinstance(args[0], torch.Tensor) else None
+    if device is not None and device.type == "cuda" and device.index != torch.cuda.current_device():
+        with torch.cuda.device(device):
+            return _render_samples_impl(n, args)
+    return _render_samples_impl(n, args)
+
+
+def _render_samples_impl(n: int, args):
+    device, g, c, s, h, (width, height), keep = _prepare(*args)
+    _check(not s.use_gps and not s.spatial_reuse and s.temporal_mode in (0, 1),
+           "render_samples needs stochastic transparency without spatial reuse, Reset or Static mode")
+    opts = dict(dtype=torch.float32, device=device)
+    outs = (torch.empty((height, width, 3), **opts), torch.empty((height, width, 1), **opts),
+            torch.empty((height, width, 1), **opts), torch.empty((height, width, 1), **opts))
+    o = _abi.Outputs(*(t.data_ptr() for t in outs))
+    ws_bytes = int(_lib.sgs_samples_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), n))
+    if ws_bytes == 0:
+        raise RuntimeError(_abi.last_error(_lib) or "invalid render arguments")
+    workspace = torch.empty((ws_bytes,), dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    status = _lib.sgs_render_samples(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h),
+                                     ctypes.byref(o), n, ctypes.c_void_p(workspace.data_ptr()),
+                                     ctypes.c_size_t(ws_bytes), ctypes.c_void_p(stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_render_samples failed ({status}): {_abi.last_error(_lib)}")
+    del keep
+    return outs
+
+
 def workspace_size(*args) -> int:
     """Bytes of scratch a render with these 29 `render` arguments needs (sgs_workspace_size)."""
     _, g, c, s, _, _, _ = _prepare(*args)

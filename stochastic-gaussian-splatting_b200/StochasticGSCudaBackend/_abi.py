@@ -122,6 +122,11 @@ SIGNATURES = {
     "sgs_render_split": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC),
                                         ctypes.POINTER(HistoryC), ctypes.POINTER(Outputs), ctypes.c_void_p,
                                         ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_samples_workspace_size": (ctypes.c_size_t, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
+                                                   ctypes.POINTER(SettingsC), ctypes.c_uint32]),
+    "sgs_render_samples": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC),
+                                          ctypes.POINTER(HistoryC), ctypes.POINTER(Outputs), ctypes.c_uint32,
+                                          ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     "sgs_render_no_alloc": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
                                            ctypes.POINTER(SettingsC), ctypes.POINTER(HistoryC),
                                            ctypes.POINTER(Outputs), ctypes.c_void_p]),

@@ -159,7 +159,7 @@ __device__ __forceinline__ void red_min_if(unsigned long long* address, const un
 // Each lane walks segment `seg` of `1 << log_segs` equal parts of the span of its row y (when
 // valid), two pixels per step; the warp takes as many steps as its longest segment needs
 // (scatter_utils.cuh:35-46 per pixel).
-template <bool kBlue, bool kHybrid>
+template <bool kBlue, bool kHybrid, bool kMulti>
 __device__ __forceinline__ void walk_rows(const AccumulateParams& a, const FrameRng& rng, const bool valid,
                                           const RowGaussian& G, const uint32_t y, const uint32_t seg = 0,
                                           const uint32_t log_segs = 0) {
@@ -200,16 +200,39 @@ __device__ __forceinline__ void walk_rows(const AccumulateParams& a, const Frame
         const float2 alpha =
             f2_unpack(f2_mul(opacity2, f2_pack(exp2f(fminf(e.x, 0.0f)), exp2f(fminf(e.y, 0.0f)))));
         const uint32_t x0 = xs + i;
-        float2 u;
-        if (kBlue) {
-            u = make_float2(st_blue_threshold(rng, seed, x0, bx), st_blue_threshold(rng, seed, x0 + 1u, bx));
+        if (!kMulti) {
+            float2 u;
+            if (kBlue) {
+                u = make_float2(st_blue_threshold(rng, seed, x0, bx), st_blue_threshold(rng, seed, x0 + 1u, bx));
+            } else {
+                u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed, x0)),
+                                             __uint_as_float(st_threshold_bits(seed, x0 + 1u))),
+                                     f2_pack(1.0f, 1.0f)));
+            }
+            red_min_if(row + i, key, i < len && alpha.x >= kMinAlpha && u.x < alpha.x);
+            red_min_if(row + i + 1u, key, i + 1u < len && alpha.y >= kMinAlpha && u.y < alpha.y);
         } else {
-            u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed, x0)),
-                                         __uint_as_float(st_threshold_bits(seed, x0 + 1u))),
-                                 f2_pack(1.0f, 1.0f)));
+            // the same two pixels in every sample of the call: alpha once, one threshold per frame
+            const bool in_x = i < len && alpha.x >= kMinAlpha;
+            const bool in_y = i + 1u < len && alpha.y >= kMinAlpha;
+            unsigned long long* row_s = row;
+            for (uint32_t sm = 0; sm < a.n_samples; ++sm, row_s += a.fb_stride) {
+                const uint32_t frame = rng.frame + sm;
+                float2 u;
+                if (kBlue) {
+                    const FrameRng rs = frame_rng_at(a, frame);
+                    u = make_float2(st_blue_threshold(rs, seed, x0, bx), st_blue_threshold(rs, seed, x0 + 1u, bx));
+                } else {
+                    // row seeds differ between frames only in the frame term
+                    const uint32_t seed_s = seed ^ ((rng.frame * 1973u) ^ (frame * 1973u));
+                    u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed_s, x0)),
+                                                 __uint_as_float(st_threshold_bits(seed_s, x0 + 1u))),
+                                         f2_pack(1.0f, 1.0f)));
+                }
+                red_min_if(row_s + i, key, in_x && u.x < alpha.x);
+                red_min_if(row_s + i + 1u, key, in_y && u.y < alpha.y);
+            }
         }
-        red_min_if(row + i, key, i < len && alpha.x >= kMinAlpha && u.x < alpha.x);
-        red_min_if(row + i + 1u, key, i + 1u < len && alpha.y >= kMinAlpha && u.y < alpha.y);
         fx = f2_add(fx, two);
     }
 }
@@ -223,16 +246,16 @@ __device__ __forceinline__ uint32_t log_chunk_rows(const uint32_t w) {
 
 // Rows [r0, r0 + (1 << log_rows)) of G, clipped to r_end: lane l walks segment l >> log_rows of row
 // r0 + (l & (rows - 1)).
-template <bool kBlue, bool kHybrid>
+template <bool kBlue, bool kHybrid, bool kMulti>
 __device__ __forceinline__ void walk_chunk(const AccumulateParams& a, const FrameRng& rng, const uint32_t lane,
                                            const RowGaussian& G, const uint32_t r0, const uint32_t log_rows,
                                            const uint32_t r_end) {
     const uint32_t r = r0 + (lane & ((1u << log_rows) - 1u));
-    walk_rows<kBlue, kHybrid>(a, rng, r < r_end, G, G.y_min + r, lane >> log_rows, 5u - log_rows);
+    walk_rows<kBlue, kHybrid, kMulti>(a, rng, r < r_end, G, G.y_min + r, lane >> log_rows, 5u - log_rows);
 }
 
 // One thread per Gaussian (accumulate_scatter.cu:19-77 for the projection and the AABB).
-template <bool kBlue, bool kHybrid>
+template <bool kBlue, bool kHybrid, bool kMulti>
 __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateParams a) {
     __shared__ RowGaussian s_gauss[kWarpsPerBlock][32];
     __shared__ uint32_t s_rank[kWarpsPerBlock][32];
@@ -341,7 +364,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         const bool valid = r < total_rows;
         const RowGaussian rg = s_gauss[wib][valid ? owner : 0];
         const uint32_t y = rg.y_min + (r - rg.row_first);
-        walk_rows<kBlue, kHybrid>(a, rng, valid, rg, y);
+        walk_rows<kBlue, kHybrid, kMulti>(a, rng, valid, rg, y);
     }
 
     // queue overflow: the warp processes its kept large Gaussians, 32 rows at a time
@@ -354,12 +377,13 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         if (lane == src) s_gauss[wib][0] = G;
         __syncwarp();
         const RowGaussian bg = s_gauss[wib][0];
-        for (uint32_t r0 = 0; r0 < bh; r0 += 32) walk_rows<kBlue, kHybrid>(a, rng, r0 + lane < bh, bg, bg.y_min + r0 + lane);
+        for (uint32_t r0 = 0; r0 < bh; r0 += 32)
+            walk_rows<kBlue, kHybrid, kMulti>(a, rng, r0 + lane < bh, bg, bg.y_min + r0 + lane);
     }
 }
 
 // Persistent consumer of the large-Gaussian queue: each warp steals one chunk of rows at a time.
-template <bool kBlue, bool kHybrid>
+template <bool kBlue, bool kHybrid, bool kMulti>
 __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams a) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long packed = a.queue->packed;
@@ -407,7 +431,7 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
             if (lane == 0) atomicOr(&a.queue->error, 1u);
             continue;
         }
-        walk_chunk<kBlue, kHybrid>(a, rng, lane, G, r0, log_rpc, m.y);
+        walk_chunk<kBlue, kHybrid, kMulti>(a, rng, lane, G, r0, log_rpc, m.y);
     }
 }
 
@@ -429,10 +453,19 @@ __global__ void clear_kernel(unsigned long long* __restrict__ fb, const size_t n
     }
 }
 
-template <bool kBlue, bool kHybrid>
+template <bool kBlue, bool kHybrid, bool kMulti>
 void launch_st(const AccumulateParams& p, const unsigned grid, const unsigned queue_grid, cudaStream_t stream) {
-    st_scatter_kernel<kBlue, kHybrid><<<grid, kBlock, 0, stream>>>(p);
-    st_queue_kernel<kBlue, kHybrid><<<queue_grid, kBlock, 0, stream>>>(p);
+    st_scatter_kernel<kBlue, kHybrid, kMulti><<<grid, kBlock, 0, stream>>>(p);
+    st_queue_kernel<kBlue, kHybrid, kMulti><<<queue_grid, kBlock, 0, stream>>>(p);
+}
+
+template <bool kMulti>
+void launch_st_variant(const AccumulateParams& p, const unsigned grid, const unsigned queue_grid, cudaStream_t stream) {
+    const bool blue = p.blue_noise != nullptr;
+    if (blue && p.hybrid) launch_st<true, true, kMulti>(p, grid, queue_grid, stream);
+    else if (blue) launch_st<true, false, kMulti>(p, grid, queue_grid, stream);
+    else if (p.hybrid) launch_st<false, true, kMulti>(p, grid, queue_grid, stream);
+    else launch_st<false, false, kMulti>(p, grid, queue_grid, stream);
 }
 
 }  // namespace
@@ -451,11 +484,8 @@ cudaError_t launch_accumulate_st(const AccumulateParams& p, const int num_sms, c
     if (p.n == 0) return cudaSuccess;
     const unsigned grid = (p.n + kBlock - 1) / kBlock;
     const unsigned queue_grid = static_cast<unsigned>(num_sms) * kQueueBlocksPerSM;
-    const bool blue = p.blue_noise != nullptr;
-    if (blue && p.hybrid) launch_st<true, true>(p, grid, queue_grid, stream);
-    else if (blue) launch_st<true, false>(p, grid, queue_grid, stream);
-    else if (p.hybrid) launch_st<false, true>(p, grid, queue_grid, stream);
-    else launch_st<false, false>(p, grid, queue_grid, stream);
+    if (p.n_samples > 1) launch_st_variant<true>(p, grid, queue_grid, stream);
+    else launch_st_variant<false>(p, grid, queue_grid, stream);
     return cudaGetLastError();
 }
 

@@ -30,6 +30,7 @@ std::atomic<uint32_t> g_queue_limit{0};
 constexpr size_t kAlign = 256;
 constexpr uint32_t kDefaultMaxBinned = 1u << 20;     // accumulate_hybrid_gps.cu:22
 constexpr uint32_t kStQueueCapacity = 1u << 18;       // large ST Gaussians held by the queue
+constexpr uint32_t kMaxSamplesPerCall = 1024;         // sgs_render_samples
 constexpr int kMaxDevices = 64;
 std::atomic<int> g_sm_count[kMaxDevices];
 
@@ -102,14 +103,14 @@ struct FullLayout {
     size_t q_key, q_geom, q_geom2, q_meta, q_count;
 };
 
-FullLayout make_layout(const Derived& d, const sgs_settings* s) {
+FullLayout make_layout(const Derived& d, const sgs_settings* s, const uint32_t n_samples = 1) {
     FullLayout F{};
     sgs_workspace_layout& L = F.pub;
     size_t off = 0;
     L.queue = off;
     off = align_up(off + sizeof(WorkQueue));
-    L.framebuffer = off;
-    off = align_up(off + d.n_fb * sizeof(unsigned long long));
+    L.framebuffer = off;  // n_samples framebuffers of n_fb keys, back to back
+    off = align_up(off + d.n_fb * n_samples * sizeof(unsigned long long));
     L.samples = off;
     off = align_up(off + d.n_fb * sizeof(float4));
     L.reuse_weights = off;
@@ -200,17 +201,24 @@ namespace {
 // Event between the accumulate and the resolve stream of split renders (one per host thread).
 thread_local cudaEvent_t t_split_event = nullptr;
 
-__global__ void advance_frame_kernel(uint32_t* frame_counter) { *frame_counter += 1u; }
+__global__ void advance_frame_kernel(uint32_t* frame_counter, const uint32_t n) { *frame_counter += n; }
 
 // The render of sgs_render / sgs_render_split: clear and accumulate on `acc_stream`, sample and
 // resolve on `res_stream` (the same stream for sgs_render).
 int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, const sgs_history* h,
                       const sgs_outputs* o, void* workspace, size_t workspace_bytes, cudaStream_t acc_stream,
-                      cudaStream_t res_stream) {
+                      cudaStream_t res_stream, const uint32_t n_samples = 1) {
     t_last_error.clear();
     Derived d;
     int st = derive(g, c, s, d);
     if (st != SGS_OK) return st;
+    if (n_samples == 0 || n_samples > kMaxSamplesPerCall)
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "%u samples per call (1 to %u)", n_samples, kMaxSamplesPerCall);
+    if (n_samples > 1 && (s->use_gps || s->spatial_reuse || s->temporal_mode == SGS_TEMPORAL_REPROJECT))
+        return fail(SGS_ERROR_INVALID_ARGUMENT,
+                    "several samples per call need stochastic transparency without spatial reuse, Reset or Static");
+    if (static_cast<uint64_t>(d.n_fb) * n_samples > 0xffffffffull)
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "the samples' framebuffers exceed 2^32 pixels");
     if (h == nullptr || o == nullptr) return fail(SGS_ERROR_INVALID_ARGUMENT, "null history or outputs");
     if (s->temporal_mode < SGS_TEMPORAL_RESET || s->temporal_mode > SGS_TEMPORAL_REPROJECT)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "invalid temporal mode %d", s->temporal_mode);
@@ -232,7 +240,7 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     if (s->spatial_reuse && (!h->k_buffer_primitives || !h->k_buffer_occlusion || !aligned16(h->k_buffer_occlusion) ||
                              (reinterpret_cast<uintptr_t>(h->k_buffer_primitives) & 7u) != 0))
         return fail(SGS_ERROR_INVALID_ARGUMENT, "spatial reuse needs aligned k-buffer arrays");
-    const FullLayout F = make_layout(d, s);
+    const FullLayout F = make_layout(d, s, n_samples);
     const sgs_workspace_layout& L = F.pub;
     if (workspace == nullptr || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)) != 0)
         return fail(SGS_ERROR_WORKSPACE, "workspace must be a 256-byte aligned device pointer");
@@ -249,7 +257,7 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     char* ws = static_cast<char*>(workspace);
     // the host counter serves calls that keep no frame index in device memory
     const uint32_t frame =
-        s->frame_index_device != nullptr ? 0u : g_frame_index.fetch_add(1u, std::memory_order_relaxed);
+        s->frame_index_device != nullptr ? 0u : g_frame_index.fetch_add(n_samples, std::memory_order_relaxed);
     const int sms = sm_count();
 
     Workspace w{};
@@ -264,7 +272,7 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     w.q.count = reinterpret_cast<uint32_t*>(ws + F.q_count);
     w.q.capacity = d.queue_capacity;
 
-    cudaError_t err = launch_clear(w.framebuffer, d.n_fb, w.queue, sms, stream);
+    cudaError_t err = launch_clear(w.framebuffer, d.n_fb * n_samples, w.queue, sms, stream);
     if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "clear: %s", cudaGetErrorString(err));
 
     const PassCamera cam = pass_camera(c, s, d.ss);
@@ -287,6 +295,8 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
         ap.hybrid = s->hybrid_scheduling != 0;
         ap.queue = w.queue;
         ap.q = w.q;
+        ap.n_samples = n_samples;
+        ap.fb_stride = d.n_fb;
         if (t_stage_start != nullptr) cudaEventRecord(t_stage_start, stream);
         err = s->use_gps ? launch_accumulate_gps(ap, sms, stream) : launch_accumulate_st(ap, sms, stream);
         if (t_stage_end != nullptr && err == cudaSuccess) err = cudaEventRecord(t_stage_end, stream);
@@ -331,11 +341,13 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     rp.sh_vec4 = g->sh_bases == 16 && aligned16(g->sh_coefficients);
     rp.frame_counter = s->frame_index_device;
     rp.temporal_mode = s->temporal_mode;
+    rp.n_samples = n_samples;
+    rp.fb_stride = d.n_fb;
     if (split) {
         // the next call's accumulate pass may start before this resolve: advance the device-resident
         // frame index behind this accumulate pass instead
         if (s->frame_index_device != nullptr) {
-            advance_frame_kernel<<<1, 1, 0, acc_stream>>>(s->frame_index_device);
+            advance_frame_kernel<<<1, 1, 0, acc_stream>>>(s->frame_index_device, n_samples);
             rp.frame_counter = nullptr;
         }
         err = cudaEventRecord(t_split_event, acc_stream);
@@ -363,6 +375,20 @@ int sgs_render_split(const sgs_gaussians* g, const sgs_camera* c, const sgs_sett
                      void* resolve_stream) {
     return render_on_streams(g, c, s, h, o, workspace, workspace_bytes, static_cast<cudaStream_t>(accumulate_stream),
                              static_cast<cudaStream_t>(resolve_stream));
+}
+
+size_t sgs_samples_workspace_size(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s,
+                                  uint32_t n_samples) {
+    Derived d;
+    if (derive(g, c, s, d) != SGS_OK || n_samples == 0 || n_samples > kMaxSamplesPerCall) return 0;
+    return make_layout(d, s, n_samples).pub.total;
+}
+
+int sgs_render_samples(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, const sgs_history* h,
+                       const sgs_outputs* o, uint32_t n_samples, void* workspace, size_t workspace_bytes,
+                       void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return render_on_streams(g, c, s, h, o, workspace, workspace_bytes, st, st, n_samples);
 }
 
 void sgs_set_queue_limit(uint32_t max_entries) { g_queue_limit.store(max_entries, std::memory_order_relaxed); }

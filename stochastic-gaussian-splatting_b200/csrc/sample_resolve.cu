@@ -405,9 +405,86 @@ __global__ void __launch_bounds__(kBlock) sample_resolve_fused_kernel(const Reso
     a.weight_mass[pixel] = weight_mass;
 }
 
+// Several samples of one call merged in order (the first in the call's temporal mode, Reset or
+// Static, the rest Static): per pixel the same box filter and the same merge as
+// sample_resolve_fused_kernel once per sample, the history carried in registers between samples, so
+// the outputs equal those of one call per sample bit for bit.
+__global__ void __launch_bounds__(kBlock) samples_resolve_kernel(const ResolveParams a) {
+    if (a.frame_counter != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.frame_counter += a.n_samples;
+    const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = idx < a.n_pixels;
+    const uint32_t pixel = active ? idx : a.n_pixels - 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ss = a.ss;
+    const uint32_t bx = (pixel % a.width) * ss;
+    const uint32_t by = (pixel / a.width) * ss;
+    const uint32_t fbw = a.width * ss;
+    const float norm = 1.0f / static_cast<float>(ss * ss);
+
+    float3 color = make_float3(0.0f, 0.0f, 0.0f);
+    float depth = 0.0f, alpha = 0.0f, weight_mass = 0.0f;
+    if (a.temporal_mode == 1 && active) {
+        color = make_float3(a.hist_image[3 * pixel + 0], a.hist_image[3 * pixel + 1], a.hist_image[3 * pixel + 2]);
+        depth = a.hist_depth[pixel];
+        alpha = a.hist_alpha[pixel];
+        weight_mass = a.hist_weight_mass[pixel];
+    }
+    for (uint32_t sm = 0; sm < a.n_samples; ++sm) {
+        const unsigned long long* fb = a.framebuffer + sm * a.fb_stride;
+        float3 cs = make_float3(0.0f, 0.0f, 0.0f);
+        float ds = 0.0f, as = 0.0f, ws = 0.0f;
+        for (uint32_t oy = 0; oy < ss; ++oy) {
+            for (uint32_t ox = 0; ox < ss; ++ox) {
+                const uint32_t fi = (by + oy) * fbw + bx + ox;
+                const float4 smp = warp_sample(a, fb[fi], lane);
+                const float wsum = 1.0f;
+                const float rcp = 1.0f / wsum;
+                cs.x += smp.x * rcp;
+                cs.y += smp.y * rcp;
+                cs.z += smp.z * rcp;
+                ds += smp.w * rcp;
+                as += (smp.w > 0.0f ? 1.0f : 0.0f) * rcp;
+                ws += wsum;
+            }
+        }
+        cs.x *= norm;
+        cs.y *= norm;
+        cs.z *= norm;
+        ds *= norm;
+        as *= norm;
+        ws *= norm;
+        if (sm == 0 && a.temporal_mode == 0) {
+            color = cs;
+            depth = ds;
+            alpha = as;
+            weight_mass = ws;
+        } else {
+            const float hm = weight_mass;
+            weight_mass = hm + ws;
+            const float hf = hm / weight_mass;
+            color.x = cs.x + hf * (color.x - cs.x);
+            color.y = cs.y + hf * (color.y - cs.y);
+            color.z = cs.z + hf * (color.z - cs.z);
+            depth = ds + hf * (depth - ds);
+            alpha = as + hf * (alpha - as);
+        }
+    }
+    if (!active) return;
+    a.image[3 * pixel + 0] = color.x;
+    a.image[3 * pixel + 1] = color.y;
+    a.image[3 * pixel + 2] = color.z;
+    a.depth[pixel] = depth;
+    a.alpha[pixel] = alpha;
+    a.weight_mass[pixel] = weight_mass;
+}
+
 }  // namespace
 
 cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream) {
+    if (p.n_samples > 1) {
+        samples_resolve_kernel<<<(p.n_pixels + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+        return cudaGetLastError();
+    }
     if (!p.spatial_reuse && p.temporal_mode != 2) {
         sample_resolve_fused_kernel<<<(p.n_pixels + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
         return cudaGetLastError();

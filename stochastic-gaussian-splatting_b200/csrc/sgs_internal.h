@@ -59,6 +59,8 @@ struct AccumulateParams {
     bool hybrid;                      // hybrid scheduling
     WorkQueue* queue;
     QueueArrays q;
+    uint32_t n_samples;               // samples of one call (frames frame .. frame + n_samples - 1)
+    size_t fb_stride;                 // framebuffer elements between consecutive samples' framebuffers
 };
 
 // Frame-dependent random-number state of one call: the frame index (from device memory when the
@@ -69,14 +71,19 @@ struct FrameRng {
     uint32_t rotation;
 };
 
-__device__ __forceinline__ FrameRng frame_rng(const AccumulateParams& a) {
+// The random-number state of frame `frame`.
+__device__ __forceinline__ FrameRng frame_rng_at(const AccumulateParams& a, const uint32_t frame) {
     FrameRng r;
-    r.frame = a.frame_ptr != nullptr ? *a.frame_ptr : a.frame_idx;
+    r.frame = frame;
     r.slice = a.blue_noise != nullptr
-                  ? a.blue_noise + static_cast<size_t>(r.frame % kBlueNoiseDepth) * kBlueNoiseWidth * kBlueNoiseHeight
+                  ? a.blue_noise + static_cast<size_t>(frame % kBlueNoiseDepth) * kBlueNoiseWidth * kBlueNoiseHeight
                   : nullptr;
-    r.rotation = (r.frame / kBlueNoiseDepth) * 0x9E3779B9u;
+    r.rotation = (frame / kBlueNoiseDepth) * 0x9E3779B9u;
     return r;
+}
+
+__device__ __forceinline__ FrameRng frame_rng(const AccumulateParams& a) {
+    return frame_rng_at(a, a.frame_ptr != nullptr ? *a.frame_ptr : a.frame_idx);
 }
 
 cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue* queue, int num_sms,
@@ -116,6 +123,8 @@ struct ResolveParams {
     bool sh_vec4;    // degree-3 SH at a 16-byte aligned base: winners load their coefficients as float4
     uint32_t* frame_counter;  // device-resident frame index advanced by the last pass, or null
     int temporal_mode;
+    uint32_t n_samples;       // samples merged by one call (the first in temporal_mode, the rest Static)
+    size_t fb_stride;         // framebuffer elements between consecutive samples' framebuffers
 };
 
 cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream);
