@@ -209,6 +209,17 @@ int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_ca
                                     const float* grad_depth, float weight, uint32_t n_samples, int first,
                                     void* scratch, void* backward_workspace, void* stream);
 
+/* Steps a and b in one call for S samples rendered by one sgs_render_samples call: `framebuffers`
+ * points at that call's S framebuffers (the workspace's framebuffer section, consecutive, one key per
+ * framebuffer pixel each); the winners' colours are recomputed per Gaussian (the same function the
+ * sample pass evaluates) instead of read from a render workspace. Same scratch, weight, `first` and
+ * sgs_backward_finish as above. */
+int sgs_backward_accumulate_framebuffers(const sgs_gaussians* gaussians, const sgs_camera* camera,
+                                         const sgs_settings* settings, const void* framebuffers, uint32_t n_samples,
+                                         const float* grad_image, const float* grad_alpha, const float* grad_depth,
+                                         float weight, int first, void* scratch, void* backward_workspace,
+                                         void* stream);
+
 /* ---- Learned resolve (no counterpart in the reference) ------------------------------------------
  * A 6-layer 3x3 convolutional denoiser (8 -> 32 -> 32 -> 32 -> 32 -> 32 -> 3, ReLU between layers,
  * the last layer adds the mean colour back) that maps a few samples' features to the converged

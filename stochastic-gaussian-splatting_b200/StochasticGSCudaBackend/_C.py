@@ -234,6 +234,16 @@ def render_samples(n_samples: int, *args):
     `render`, frames f .. f + n_samples - 1 merged in order (the first in the given temporal mode,
     Reset or Static, the rest Static); returns the final (image, depth, alpha, weight_mass), equal
     bit for bit to `n_samples` `render` calls. Stochastic transparency without spatial reuse."""
+    return _render_samples(n_samples, args, want_workspace=False)
+
+
+def render_samples_with_workspace(n_samples: int, *args):
+    """As `render_samples`, plus the workspace (its framebuffer section holds the n_samples winner
+    framebuffers back to back) and its layout."""
+    return _render_samples(n_samples, args, want_workspace=True)
+
+
+def _render_samples(n_samples: int, args, want_workspace: bool):
     if len(args) != 29:
         raise TypeError(f"render_samples() takes n_samples and 29 render arguments ({len(args)} given)")
     n = int(n_samples)
@@ -241,11 +251,11 @@ def render_samples(n_samples: int, *args):
     device = args[0].device if isinstance(args[0], torch.Tensor) else None
     if device is not None and device.type == "cuda" and device.index != torch.cuda.current_device():
         with torch.cuda.device(device):
-            return _render_samples_impl(n, args)
-    return _render_samples_impl(n, args)
+            return _render_samples_impl(n, args, want_workspace)
+    return _render_samples_impl(n, args, want_workspace)
 
 
-def _render_samples_impl(n: int, args):
+def _render_samples_impl(n: int, args, want_workspace: bool):
     device, g, c, s, h, (width, height), keep = _prepare(*args)
     _check(not s.use_gps and not s.spatial_reuse and s.temporal_mode in (0, 1),
            "render_samples needs stochastic transparency without spatial reuse, Reset or Static mode")
@@ -264,7 +274,11 @@ def _render_samples_impl(n: int, args):
     if status != _abi.SGS_OK:
         raise RuntimeError(f"sgs_render_samples failed ({status}): {_abi.last_error(_lib)}")
     del keep
-    return outs
+    if not want_workspace:
+        return outs
+    layout = _abi.WorkspaceLayout()
+    _lib.sgs_get_workspace_layout(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(layout))
+    return outs, workspace, layout
 
 
 def workspace_size(*args) -> int:

@@ -149,6 +149,11 @@ SIGNATURES = {
                                                        ctypes.POINTER(SettingsC), ctypes.c_void_p, ctypes.c_void_p,
                                                        ctypes.c_void_p, ctypes.c_float, ctypes.c_uint32, ctypes.c_int,
                                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_backward_accumulate_framebuffers": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
+                                                            ctypes.POINTER(SettingsC), ctypes.c_void_p, ctypes.c_uint32,
+                                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                            ctypes.c_float, ctypes.c_int, ctypes.c_void_p,
+                                                            ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_conv3x3_weights_size": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     "sgs_conv3x3": (ctypes.c_int, [ctypes.POINTER(Conv3x3Args), ctypes.c_void_p]),
     "sgs_conv3x3_wgrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,

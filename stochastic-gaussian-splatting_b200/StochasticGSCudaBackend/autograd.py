@@ -7,12 +7,14 @@ backward pass to all five parameter tensors (the reference renders only; it has 
 
 The backward is an unbiased estimator of the gradient of the expected image (see
 csrc/backward_st.cu): each sample's winners give a one-sample estimate, averaged over the samples.
-Winners are either kept from the forward pass (`store_winners=True`, 24 bytes per framebuffer pixel
-and sample) or recomputed by rendering the same frame indices again (`store_winners=False`: one more
-render per sample, no render workspace kept per sample). Either way the backward first tabulates
-every sample's winner and colour term (12 bytes per framebuffer pixel and sample, 8 more per pixel) and then walks
-the Gaussians' fragments once for all samples (sgs_backward_sample_terms,
-sgs_backward_accumulate_samples).
+The forward renders all samples in one call (`_C.render_samples`: one fragment walk, the samples'
+winner framebuffers side by side in its workspace, outputs bit-identical to one call per sample).
+Winners are either kept from the forward pass (`store_winners=True`, 8 bytes per framebuffer pixel
+and sample) or recomputed in backward by rendering the same frame indices again
+(`store_winners=False`: one more multi-sample render, nothing kept between the passes). The backward
+tabulates every sample's winner and colour term (12 bytes per framebuffer pixel and sample, 8 more
+per pixel) and walks the Gaussians' fragments once for all samples
+(sgs_backward_accumulate_framebuffers).
 """
 from __future__ import annotations
 
@@ -47,6 +49,23 @@ def _render_one(tensors, settings: Settings, hist, mode: int, frame: int):
                                     *kb, *hist, torch.eye(4, device=dev), mode)
 
 
+def _render_all(tensors, settings: Settings, n_samples: int, first_frame: int):
+    """n_samples samples (Reset, then Static) in one call; returns (outputs, workspace, layout) and
+    leaves the process-wide frame index where it was."""
+    saved = _C.get_frame_index()
+    _C.set_frame_index(first_frame)
+    try:
+        n_fb = settings.width * settings.height * max(1, settings.supersampling_factor) ** 2
+        dev = tensors[0].device
+        kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device=dev), torch.empty((0, n_fb, 4), device=dev))
+        e = torch.empty(0)
+        return _C.render_samples_with_workspace(n_samples, *tensors, *settings.as_tuple(),
+                                                torch.empty(0, dtype=torch.uint8, device=dev), *kb, e, e, e, e,
+                                                torch.eye(4, device=dev), 0)
+    finally:
+        _C.set_frame_index(saved)
+
+
 class _RenderSamples(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means, scales, rotations, opacities, sh, settings, n_samples, first_frame, store_winners):
@@ -54,20 +73,12 @@ class _RenderSamples(torch.autograd.Function):
             raise RuntimeError("render_samples differentiates stochastic transparency without spatial reuse or "
                                "proper antialiasing")
         tensors = tuple(t.detach().contiguous() for t in (means, scales, rotations, opacities, sh))
-        e = torch.empty(0)
-        hist = (e, e, e, e)
-        workspaces = []
-        for s in range(n_samples):
-            outs, ws, _ = _render_one(tensors, settings, hist, 0 if s == 0 else 1, first_frame + s)
-            hist = outs
-            if store_winners:
-                workspaces.append(ws)
+        (image, depth, alpha, _), ws, layout = _render_all(tensors, settings, n_samples, first_frame)
         ctx.save_for_backward(*tensors)
         ctx.settings = settings
         ctx.n_samples = n_samples
         ctx.first_frame = first_frame
-        ctx.workspaces = workspaces
-        image, depth, alpha, _ = hist
+        ctx.winners = (ws, layout.framebuffer) if store_winners else None
         return image, depth, alpha
 
     @staticmethod
@@ -84,35 +95,27 @@ class _RenderSamples(torch.autograd.Function):
         stream = torch.cuda.current_stream(dev).cuda_stream
         weight = 1.0 / ctx.n_samples
         n = ctx.n_samples
-        # one table of every sample's winners and colour terms, then one fused walk over the fragments
+        if ctx.winners is not None:
+            ws, fb_offset = ctx.winners
+        else:
+            _, ws, layout = _render_all(tensors, settings, n, ctx.first_frame)
+            fb_offset = layout.framebuffer
         scratch = torch.empty(_lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s), n),
                               dtype=torch.uint8, device=dev)
         gptr = [None if t is None else ctypes.c_void_p(t.data_ptr()) for t in grads_in]
-        e = torch.empty(0)
-        hist = (e, e, e, e)
-        for k in range(n):
-            if ctx.workspaces:
-                ws = ctx.workspaces[k]
-            else:
-                hist, ws, _ = _render_one(tensors, settings, hist, 0 if k == 0 else 1, ctx.first_frame + k)
-            st = _lib.sgs_backward_sample_terms(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
-                                                ctypes.c_void_p(ws.data_ptr()), gptr[0], gptr[1], gptr[2],
-                                                ctypes.c_float(weight), k, n, ctypes.c_void_p(scratch.data_ptr()),
-                                                ctypes.c_void_p(stream))
-            if st != _abi.SGS_OK:
-                raise RuntimeError(f"sgs_backward_sample_terms failed ({st}): {_abi.last_error(_lib)}")
-        st = _lib.sgs_backward_accumulate_samples(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), gptr[0], gptr[1],
-                                                  gptr[2], ctypes.c_float(weight), n, 1,
-                                                  ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(bw.data_ptr()),
-                                                  ctypes.c_void_p(stream))
+        st = _lib.sgs_backward_accumulate_framebuffers(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s),
+                                                       ctypes.c_void_p(ws.data_ptr() + fb_offset), n, gptr[0],
+                                                       gptr[1], gptr[2], ctypes.c_float(weight), 1,
+                                                       ctypes.c_void_p(scratch.data_ptr()),
+                                                       ctypes.c_void_p(bw.data_ptr()), ctypes.c_void_p(stream))
         if st != _abi.SGS_OK:
-            raise RuntimeError(f"sgs_backward_accumulate_samples failed ({st}): {_abi.last_error(_lib)}")
+            raise RuntimeError(f"sgs_backward_accumulate_framebuffers failed ({st}): {_abi.last_error(_lib)}")
         outs = [torch.empty_like(t) for t in tensors]
         st = _lib.sgs_backward_finish(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(bw.data_ptr()),
                                       *(ctypes.c_void_p(t.data_ptr()) for t in outs), ctypes.c_void_p(stream))
         if st != _abi.SGS_OK:
             raise RuntimeError(f"sgs_backward_finish failed ({st}): {_abi.last_error(_lib)}")
-        ctx.workspaces = []
+        ctx.winners = None
         return (*outs, None, None, None, None)
 
 

@@ -219,6 +219,45 @@ int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_ca
     return SGS_OK;
 }
 
+int sgs_backward_accumulate_framebuffers(const sgs_gaussians* gaussians, const sgs_camera* camera,
+                                         const sgs_settings* settings, const void* framebuffers, uint32_t n_samples,
+                                         const float* grad_image, const float* grad_alpha, const float* grad_depth,
+                                         float weight, int first, void* scratch, void* backward_workspace,
+                                         void* stream_ptr) {
+    BackwardSetup S;
+    int st = setup(gaussians, camera, settings, S);
+    if (st != SGS_OK) return st;
+    if (framebuffers == nullptr || grad_image == nullptr || scratch == nullptr || backward_workspace == nullptr ||
+        (reinterpret_cast<uintptr_t>(framebuffers) & 7u) != 0 || (reinterpret_cast<uintptr_t>(scratch) & 255u) != 0 ||
+        (reinterpret_cast<uintptr_t>(backward_workspace) & 15u) != 0)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT,
+                            "null framebuffers, image gradient, scratch or backward workspace, or misaligned buffers");
+    if (n_samples == 0 || n_samples > kMaxFusedSamples)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT, "%u samples (1 to %u)", n_samples, kMaxFusedSamples);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    BackwardParams& p = S.p;
+    p.framebuffer = static_cast<const unsigned long long*>(framebuffers);
+    p.grad_image = grad_image;
+    p.grad_alpha = grad_alpha;
+    p.grad_depth = grad_depth;
+    p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
+    set_sample_table(p, scratch, n_samples);
+    set_backward_buffers(p, backward_workspace);
+    cudaError_t err = cudaSuccess;
+    if (first) err = cudaMemsetAsync(p.accum, 0, kAccumFloats * p.n * sizeof(float), stream);
+    if (err == cudaSuccess) err = launch_backward_colors(p, stream);
+    if (err == cudaSuccess) err = launch_backward_framebuffer_terms(p, stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(p.bw_queue, 0, sizeof(WorkQueue), stream);
+    if (err == cudaSuccess) {
+        int device = 0;
+        err = cudaGetDevice(&device);
+        if (err == cudaSuccess) err = cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, device);
+    }
+    if (err == cudaSuccess) err = launch_backward_fragments_samples(p, stream);
+    if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
+    return SGS_OK;
+}
+
 int sgs_backward_finish(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
                         void* backward_workspace, float* d_means, float* d_scales, float* d_rotations,
                         float* d_opacities, float* d_sh, void* stream_ptr) {

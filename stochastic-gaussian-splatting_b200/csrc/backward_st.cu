@@ -175,6 +175,33 @@ __global__ void __launch_bounds__(kBlock) sample_terms_kernel(const BackwardPara
     b.pix_max_key[pix] = b.sample == 0 ? key : max(b.pix_max_key[pix], key);
 }
 
+// The same table from the framebuffers of all S samples at once (consecutive, b.n_fb apart): the
+// winner's colour is its Gaussian's view-dependent colour (colors_kernel, the function the sample
+// pass evaluates) and its depth the key's high word.
+__global__ void __launch_bounds__(kBlock) framebuffer_terms_kernel(const BackwardParams b) {
+    const uint32_t pix = blockIdx.x * kBlock + threadIdx.x;
+    if (pix >= b.n_fb) return;
+    const uint32_t px = pix % b.cam.width_int, py = pix / b.cam.width_int;
+    const uint32_t ip = (py / b.ss) * b.width + px / b.ss;
+    const float g0 = b.grad_image[3 * ip + 0], g1 = b.grad_image[3 * ip + 1], g2 = b.grad_image[3 * ip + 2];
+    const float gd = b.grad_depth != nullptr ? b.grad_depth[ip] : 0.0f;
+    unsigned long long max_key = 0;
+    const size_t row = static_cast<size_t>(pix) * b.n_samples;
+    for (uint32_t s = 0; s < b.n_samples; ++s) {
+        const unsigned long long key = b.framebuffer[static_cast<size_t>(s) * b.n_fb + pix];
+        float t = 0.0f;
+        if (key != kEmptyFragment) {
+            const uint32_t w = static_cast<uint32_t>(key);
+            t = g0 * b.colors[3 * w + 0] + g1 * b.colors[3 * w + 1] + g2 * b.colors[3 * w + 2] +
+                gd * __uint_as_float(static_cast<uint32_t>(key >> 32));
+        }
+        b.pix_keys[row + s] = key;
+        b.pix_terms[row + s] = t * b.grad_scale;
+        max_key = max(max_key, key);
+    }
+    b.pix_max_key[pix] = max_key;
+}
+
 // Rows per chunk of a queued Gaussian of AABB width w (log2): about kChunkPixels pixels, a power of
 // two between 1 and 32; each row of a chunk is walked in 32 / rows segments.
 __device__ __forceinline__ uint32_t log_chunk_rows(const uint32_t w) {
@@ -609,6 +636,12 @@ cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream)
 cudaError_t launch_backward_fragments(const BackwardParams& p, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
     fragments_backward_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_framebuffer_terms(const BackwardParams& p, cudaStream_t stream) {
+    if (p.n_fb == 0) return cudaSuccess;
+    framebuffer_terms_kernel<<<(p.n_fb + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }
 

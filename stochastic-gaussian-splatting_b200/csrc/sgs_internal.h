@@ -177,6 +177,7 @@ cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream)
 cudaError_t launch_backward_fragments(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_projection(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_sample_terms(const BackwardParams& p, cudaStream_t stream);
+cudaError_t launch_backward_framebuffer_terms(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStream_t stream);
 
 // Sets the calling thread's sgs_last_error() message (printf format) and returns `status`.

@@ -173,3 +173,58 @@ def test_fused_walk_rejects_bad_sample_counts(cuda_device):
                                        ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(gi.data_ptr()), None, None,
                                        ctypes.c_float(1.0), 4, 4, ctypes.c_void_p(scratch.data_ptr()), None)
     assert st == _abi.SGS_ERROR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("ss,n_samples,big", [(1, 6, False), (2, 5, True), (3, 4, True)])
+def test_framebuffer_walk_equals_one_walk_per_sample(ss, n_samples, big, cuda_device):
+    """sgs_backward_accumulate_framebuffers on the framebuffers of one sgs_render_samples call gives
+    the gradients of sgs_backward_accumulate called once per sample (one render call each), up to
+    float summation order."""
+    import ctypes
+
+    from StochasticGSCudaBackend import _abi, _C
+    from StochasticGSCudaBackend.autograd import _render_all, _render_one, _structs
+
+    lib = _abi.load()
+    scene, cam, gi, ga, gd = _big_problem(ss) if big else _problem(ss)
+    settings = _settings(cam, ss)
+    tensors = tuple(t.cuda().contiguous() for t in scene.tensors())
+    g, c, s = _structs(*tensors, settings)
+    grads = [torch.tensor(a, dtype=torch.float32, device="cuda").contiguous() for a in (gi, ga, gd)]
+    gp = [ctypes.c_void_p(t.data_ptr()) for t in grads]
+    e = torch.empty(0)
+    hist, workspaces = (e, e, e, e), []
+    for k in range(n_samples):
+        hist, ws, _ = _render_one(tensors, settings, hist, 0 if k == 0 else 1, 700 + k)
+        workspaces.append(ws)
+    outs, ws_all, layout = _render_all(tensors, settings, n_samples, 700)
+    for a, b in zip(outs, hist):
+        assert torch.equal(a, b)
+    weight = ctypes.c_float(1.0 / n_samples)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    nbytes = lib.sgs_backward_workspace_size(tensors[0].shape[0])
+
+    def finish(bw):
+        res = [torch.empty_like(t) for t in tensors]
+        assert lib.sgs_backward_finish(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(bw.data_ptr()),
+                                       *(ctypes.c_void_p(t.data_ptr()) for t in res), stream) == _abi.SGS_OK
+        return [t.cpu().numpy() for t in res]
+
+    bw_a = torch.empty(nbytes // 4 + 4, device="cuda")
+    for k, ws in enumerate(workspaces):
+        assert lib.sgs_backward_accumulate(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(ws.data_ptr()),
+                                           *gp, weight, int(k == 0), ctypes.c_void_p(bw_a.data_ptr()),
+                                           stream) == _abi.SGS_OK
+    per_sample = finish(bw_a)
+    bw_b = torch.empty(nbytes // 4 + 4, device="cuda")
+    scratch = torch.empty(lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s), n_samples),
+                          dtype=torch.uint8, device="cuda")
+    assert lib.sgs_backward_accumulate_framebuffers(
+        ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(ws_all.data_ptr() + layout.framebuffer),
+        n_samples, *gp, weight, 1, ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(bw_b.data_ptr()),
+        stream) == _abi.SGS_OK
+    fused = finish(bw_b)
+    for k, a, b in zip(KEYS, per_sample, fused):
+        scale = np.abs(a).max()
+        assert scale > 0, k
+        np.testing.assert_allclose(b, a, rtol=2e-3, atol=2e-5 * scale, err_msg=k)
