@@ -46,7 +46,7 @@ DEFAULT_WORKLOAD = "batch_6m_1080_st"
 
 # DRAM bytes (read + write) of one st_scatter_kernel launch on the default workload, from
 # `ncu --set full` (profiles/st_scatter_kernel_batch_6m_1080.md)
-NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 278.91e6 + 16.07e6}
+NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 279.15e6 + 15.66e6}
 
 # measured copy bandwidth and bf16 GEMM rate of this pool's B200s when MEASURED_PEAKS.json is absent
 FALLBACK_HBM_GBS = 6650.0
