@@ -364,6 +364,8 @@ def run_ours(args, world, rank, local) -> dict | None:
     if not fl["gps"]:
         line["samples_per_call"] = samples_per_call(scene, cam, fl, dev, n_samples=8, calls=max(4, args.steps // 8))
     if not args.no_batch and args.workload.startswith("batch_6m"):
+        line["camera_path"] = camera_path_fps(scene, fl, dev, spp=8)
+    if not args.no_batch and args.workload.startswith("batch_6m"):
         line["batch32_graph"] = batch_graph(scene, fl, dev, steps=max(4, args.steps // 8))
     if not (args.no_train and args.no_learned) and args.workload.startswith("batch_6m"):
         del scene
@@ -480,6 +482,22 @@ def samples_per_call(scene, cam, fl, dev, n_samples: int, calls: int) -> dict:
     ms = t0.elapsed_time(t1) / (calls * n_samples)
     return {"samples_per_call": n_samples, "ms_per_sample": round(ms, 5),
             "sample_frames_per_s": round(1000.0 / ms, 1)}
+
+
+def camera_path_fps(scene, fl, dev, spp: int, n_views: int = 16, iterations: int = 3) -> dict:
+    """The reference's FPS harness (Trainer.py:79-120: warm-up pass, then passes with a device
+    synchronisation around every frame) over 16 orbit views at 1920x1080, each frame `spp` samples
+    with the frame logic of Renderer.py:48-103 (sgs_viewer.ProgressiveRenderer; moving views reset)."""
+    import sgs_viewer
+
+    views = [sgs_viewer.View.from_camera(c, frame_idx=i)
+             for i, c in enumerate(sgs_scenes.orbit_cameras(n_views, 25.0, 1920, 1080))]
+    r = sgs_viewer.ProgressiveRenderer(*scene.tensors(), supersampling_factor=fl["ss"], use_gps=fl["gps"],
+                                       hybrid_scheduling=fl["hybrid"], samples_per_pixel=spp)
+    res = sgs_viewer.benchmark_camera_path(r, views, iterations=iterations)
+    return {"views": n_views, "resolution": "1920x1080", "samples_per_pixel": spp, "iterations": iterations,
+            "avg_fps": round(res["avg_fps"], 2), "avg_ms": round(res["avg_ms"], 4),
+            "timing": "perf_counter with a device synchronisation around every frame (Trainer.py:97-106)"}
 
 
 def batch_graph(scene, fl, dev, steps: int) -> dict:
