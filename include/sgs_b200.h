@@ -141,9 +141,10 @@ int sgs_render_split(const sgs_gaussians* gaussians, const sgs_camera* camera, c
  * Renderer.py:85-87 moved onto the device): renders n_samples samples with frame indices f .. f + n - 1
  * (f = the current frame index, which advances by n) and merges them into the history in order, the
  * first in settings->temporal_mode (Reset or Static) and the rest Static. The outputs equal those of
- * n_samples sgs_render calls bit for bit. One walk over the Gaussians' fragments evaluates each
- * fragment's alpha once and every sample's threshold, and one resolve pass reads the history once.
- * Stochastic transparency only, without spatial reuse or Reproject (SGS_ERROR_INVALID_ARGUMENT);
+ * n_samples sgs_render calls bit for bit. Stochastic transparency: one walk over the Gaussians'
+ * fragments evaluates each fragment's alpha once and every sample's threshold; GPS (scatter
+ * scheduling): one projection, then each frame's point draws; one resolve pass reads the history
+ * once. Not with spatial reuse, Reproject or hybrid GPS (SGS_ERROR_INVALID_ARGUMENT);
  * n_samples from 1 to 1024. The workspace holds sgs_samples_workspace_size(..., n_samples) bytes
  * (n_samples framebuffers). */
 size_t sgs_samples_workspace_size(const sgs_gaussians* gaussians, const sgs_camera* camera,

@@ -233,7 +233,7 @@ def render_samples(n_samples: int, *args):
     """`n_samples` samples in one call (the C ABI's sgs_render_samples): the same 29 arguments as
     `render`, frames f .. f + n_samples - 1 merged in order (the first in the given temporal mode,
     Reset or Static, the rest Static); returns the final (image, depth, alpha, weight_mass), equal
-    bit for bit to `n_samples` `render` calls. Stochastic transparency without spatial reuse."""
+    bit for bit to `n_samples` `render` calls. No spatial reuse; GPS with scatter scheduling only."""
     return _render_samples(n_samples, args, want_workspace=False)
 
 
@@ -257,8 +257,8 @@ def _render_samples(n_samples: int, args, want_workspace: bool):
 
 def _render_samples_impl(n: int, args, want_workspace: bool):
     device, g, c, s, h, (width, height), keep = _prepare(*args)
-    _check(not s.use_gps and not s.spatial_reuse and s.temporal_mode in (0, 1),
-           "render_samples needs stochastic transparency without spatial reuse, Reset or Static mode")
+    _check(not (s.use_gps and s.hybrid_scheduling) and not s.spatial_reuse and s.temporal_mode in (0, 1),
+           "render_samples needs no spatial reuse, Reset or Static mode, and for GPS scatter scheduling")
     opts = dict(dtype=torch.float32, device=device)
     outs = (torch.empty((height, width, 3), **opts), torch.empty((height, width, 1), **opts),
             torch.empty((height, width, 1), **opts), torch.empty((height, width, 1), **opts))

@@ -39,7 +39,8 @@ struct PointSource {
 };
 
 // Draws one point from `seed` and merges it (scatter_utils.cuh:116-129).
-__device__ __forceinline__ void gps_point(const AccumulateParams& a, uint2& seed, const PointSource& s) {
+__device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned long long* __restrict__ fb, uint2& seed,
+                                          const PointSource& s) {
     const float2 u = pcg2d_uniform(seed);
     const float2 xy = truncated_box_muller(u.x, u.y, s.opacity_rcp, s.opacity_dilog);
     const float sx = s.mean2d.x + s.L.x * xy.x;
@@ -51,7 +52,7 @@ __device__ __forceinline__ void gps_point(const AccumulateParams& a, uint2& seed
     if (power > s.power_threshold) return;
     const uint32_t px = __float2uint_rd(sx);
     const uint32_t py = __float2uint_rd(sy);
-    atomicMin(&a.framebuffer[py * a.cam.width_int + px], s.key);
+    atomicMin(&fb[py * a.cam.width_int + px], s.key);
 }
 
 __device__ __forceinline__ PointSource shfl_source(const PointSource& s, const uint32_t src) {
@@ -81,15 +82,9 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     PointSource s;
     s.opacity_dilog = gps_dilog(p.opacity);
     const float importance = kTwoPi * sqrtf(p.determinant) * s.opacity_dilog;
-    uint2 seed = gps_seed(g, frame_rng(a).frame);
-    const uint32_t true_count = poisson_count(seed, importance);
-    if (true_count == 0) active = false;
     const uint32_t cap = a.max_fragments != 0
                              ? a.max_fragments
                              : __float2uint_rn(a.cam.width * a.cam.height / (2.0f * a.cam.ss * a.cam.ss));
-    const uint32_t count = min(true_count, cap);
-    if (__ballot_sync(kFullMask, active) == 0) return;
-
     const float c0 = sqrtf(p.cov2d.x);
     const float c1 = p.cov2d.y / c0;
     const float c2 = sqrtf(p.cov2d.z - c1 * c1);
@@ -99,56 +94,70 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     s.power_threshold = p.power_threshold;
     s.opacity_rcp = 1.0f / fmaxf(p.opacity, 1.0e-37f);
     s.key = pack_fragment(p.depth, g);
+    const bool projected = active;
+    const uint32_t frame0 = frame_rng(a).frame;
+    // several samples of one call (scatter scheduling only): the projection once, then each frame's
+    // own point draws into its own framebuffer
+    const uint32_t n_frames = a.hybrid ? 1u : a.n_samples;
+    for (uint32_t sm = 0; sm < n_frames; ++sm) {
+        unsigned long long* fb = a.framebuffer + sm * a.fb_stride;
+        // every lane, culled or padding, draws its Poisson sample (accumulate_scatter.cu:104-124)
+        uint2 seed = gps_seed(g, frame0 + sm);
+        const uint32_t true_count = poisson_count(seed, importance);
+        bool act = projected && true_count != 0;
+        const uint32_t count = min(true_count, cap);
+        if (__ballot_sync(kFullMask, act) == 0) continue;
 
-    if (a.hybrid) {
-        // bin Gaussians with many points: one 64-bit atomic per warp reserves entries and chunks
-        const bool want = active && count > kBinningPointThreshold;
-        const uint32_t ballot = __ballot_sync(kFullMask, want);
-        if (ballot != 0) {
-            const uint32_t chunks = want ? (count + kChunkPoints - 1) / kChunkPoints : 0u;
-            uint32_t incl = chunks;
+        if (a.hybrid) {
+            // bin Gaussians with many points: one 64-bit atomic per warp reserves entries and chunks
+            const bool want = act && count > kBinningPointThreshold;
+            const uint32_t ballot = __ballot_sync(kFullMask, want);
+            if (ballot != 0) {
+                const uint32_t chunks = want ? (count + kChunkPoints - 1) / kChunkPoints : 0u;
+                uint32_t incl = chunks;
 #pragma unroll
-            for (uint32_t o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(kFullMask, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const uint32_t warp_chunks = __shfl_sync(kFullMask, incl, 31);
-            const uint32_t leader = __ffs(ballot) - 1;
-            unsigned long long base = 0;
-            if (lane == leader)
-                base = atomicAdd(&a.queue->packed,
-                                 (static_cast<unsigned long long>(__popc(ballot)) << kQueueEntryShift) | warp_chunks);
-            base = __shfl_sync(kFullMask, base, leader);
-            const uint32_t e = static_cast<uint32_t>(base >> kQueueEntryShift) + __popc(ballot & ((1u << lane) - 1u));
-            const unsigned long long first_chunk = (base & kQueueChunkMask) + (incl - chunks);
-            if (want && e < a.max_binned && e < a.q.capacity && first_chunk + chunks <= 0xffffffffull) {
-                a.q.key[e] = s.key;
-                a.q.geom[e] = make_float4(s.mean2d.x, s.mean2d.y, s.L.x, s.L.y);
-                a.q.geom2[e] = make_float4(s.L.z, s.power_threshold, s.opacity_rcp, s.opacity_dilog);
-                a.q.meta[e] = make_uint4(__float_as_uint(s.conic.x), __float_as_uint(s.conic.y),
-                                         __float_as_uint(s.conic.z), static_cast<uint32_t>(first_chunk));
-                a.q.count[e] = count;
-                active = false;
+                for (uint32_t o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFullMask, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const uint32_t warp_chunks = __shfl_sync(kFullMask, incl, 31);
+                const uint32_t leader = __ffs(ballot) - 1;
+                unsigned long long base = 0;
+                if (lane == leader)
+                    base = atomicAdd(&a.queue->packed,
+                                     (static_cast<unsigned long long>(__popc(ballot)) << kQueueEntryShift) | warp_chunks);
+                base = __shfl_sync(kFullMask, base, leader);
+                const uint32_t e = static_cast<uint32_t>(base >> kQueueEntryShift) + __popc(ballot & ((1u << lane) - 1u));
+                const unsigned long long first_chunk = (base & kQueueChunkMask) + (incl - chunks);
+                if (want && e < a.max_binned && e < a.q.capacity && first_chunk + chunks <= 0xffffffffull) {
+                    a.q.key[e] = s.key;
+                    a.q.geom[e] = make_float4(s.mean2d.x, s.mean2d.y, s.L.x, s.L.y);
+                    a.q.geom2[e] = make_float4(s.L.z, s.power_threshold, s.opacity_rcp, s.opacity_dilog);
+                    a.q.meta[e] = make_uint4(__float_as_uint(s.conic.x), __float_as_uint(s.conic.y),
+                                             __float_as_uint(s.conic.z), static_cast<uint32_t>(first_chunk));
+                    a.q.count[e] = count;
+                    act = false;
+                }
             }
         }
-    }
 
-    // own first points, sequentially per lane
-    for (uint32_t i = 0; active && i < count && i < kSequentialFragments; ++i) gps_point(a, seed, s);
+        // own first points, sequentially per lane
+        for (uint32_t i = 0; act && i < count && i < kSequentialFragments; ++i) gps_point(a, fb, seed, s);
 
-    // the rest cooperatively, one large Gaussian at a time in lane order, each lane on its own seed
-    const uint32_t coop = __ballot_sync(kFullMask, active && count > kSequentialFragments);
-    uint32_t pending = coop;
-    while (pending) {
-        const uint32_t src = __ffs(pending) - 1;
-        pending &= pending - 1;
-        const uint32_t n_src = __shfl_sync(kFullMask, count, src);
-        const PointSource t = shfl_source(s, src);
-        const uint32_t iterations = (n_src - kSequentialFragments + 31) / 32;
-        for (uint32_t it = 0; it < iterations; ++it) {
-            const uint32_t fi = it * 32 + lane + kSequentialFragments;
-            if (fi >= n_src) continue;
-            gps_point(a, seed, t);
+        // the rest cooperatively, one large Gaussian at a time in lane order, each lane on its own seed
+        const uint32_t coop = __ballot_sync(kFullMask, act && count > kSequentialFragments);
+        uint32_t pending = coop;
+        while (pending) {
+            const uint32_t src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const uint32_t n_src = __shfl_sync(kFullMask, count, src);
+            const PointSource t = shfl_source(s, src);
+            const uint32_t iterations = (n_src - kSequentialFragments + 31) / 32;
+            for (uint32_t it = 0; it < iterations; ++it) {
+                const uint32_t fi = it * 32 + lane + kSequentialFragments;
+                if (fi >= n_src) continue;
+                gps_point(a, fb, seed, t);
+            }
         }
     }
 }
@@ -194,7 +203,7 @@ __global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParam
             if (point >= n_points) break;
             uint2 seed = base_seed;
             seed.x ^= point * 0x9E3779B9u;
-            gps_point(a, seed, s);
+            gps_point(a, a.framebuffer, seed, s);
         }
     }
 }

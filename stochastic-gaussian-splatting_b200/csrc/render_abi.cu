@@ -214,9 +214,10 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     if (st != SGS_OK) return st;
     if (n_samples == 0 || n_samples > kMaxSamplesPerCall)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "%u samples per call (1 to %u)", n_samples, kMaxSamplesPerCall);
-    if (n_samples > 1 && (s->use_gps || s->spatial_reuse || s->temporal_mode == SGS_TEMPORAL_REPROJECT))
+    if (n_samples > 1 && ((s->use_gps && s->hybrid_scheduling) || s->spatial_reuse ||
+                          s->temporal_mode == SGS_TEMPORAL_REPROJECT))
         return fail(SGS_ERROR_INVALID_ARGUMENT,
-                    "several samples per call need stochastic transparency without spatial reuse, Reset or Static");
+                    "several samples per call need no spatial reuse, Reset or Static, and for GPS scatter scheduling");
     if (static_cast<uint64_t>(d.n_fb) * n_samples > 0xffffffffull)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "the samples' framebuffers exceed 2^32 pixels");
     if (h == nullptr || o == nullptr) return fail(SGS_ERROR_INVALID_ARGUMENT, "null history or outputs");

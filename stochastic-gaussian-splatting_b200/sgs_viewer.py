@@ -8,8 +8,8 @@ available here. This module restates what those callers do, on this library:
   the pose changed or progressive rendering is disabled; STATIC when the pose is unchanged; otherwise
   REPROJECT with temporal reuse, else RESET; SAMPLES_PER_PIXEL samples, the first in that mode and
   the rest STATIC; then the background composite and the depth normalisation. The sample loop runs
-  as one `_C.render_samples` call where that path applies (stochastic transparency without spatial
-  reuse, first mode RESET or STATIC), which renders the same bits as the loop.
+  as one `_C.render_samples` call where that path applies (no spatial reuse, first mode RESET or
+  STATIC, GPS only with scatter scheduling), which renders the same bits as the loop.
 * `load_camera_path(path)` reads the camera-path .json of Trainer.py:28-65 (per frame: `rotation`
   3x3 and `position` of camera-to-world, `fx`, `fy`, `width`, `height`, `id`).
 * `benchmark_camera_path(renderer, views)` is the FPS measurement of Trainer.py:79-120: one warm-up
@@ -111,7 +111,7 @@ class ProgressiveRenderer:
 
     def _samples(self, settings: Settings, v2pv: torch.Tensor, mode: TemporalMode, n: int) -> None:
         """n samples merged into the history, the first in `mode`, the rest STATIC."""
-        one_call = (not settings.use_gps and not settings.spatial_reuse
+        one_call = (not (settings.use_gps and settings.hybrid_scheduling) and not settings.spatial_reuse
                     and mode in (TemporalMode.RESET, TemporalMode.STATIC) and n > 1)
         if one_call:
             self.history = History(*_C.render_samples(

@@ -1,7 +1,8 @@
 """Several samples in one call (sgs_render_samples) against one render call per sample (GPU).
 
-The multi-sample path walks each fragment once for all samples and merges the samples into the
-history in one resolve pass; its outputs must equal those of the same number of `_C.render` calls
+The multi-sample path walks each fragment once for all samples (stochastic transparency) or projects
+once and draws each frame's points (GPS), and merges the samples into the history in one resolve
+pass; its outputs must equal those of the same number of `_C.render` calls
 (first call in the given temporal mode, the rest Static) bit for bit, and the frame index must
 advance by the number of samples.
 """
@@ -31,6 +32,8 @@ CASES = [
     (dict(aa=False, ss=3, gps=False, hybrid=False), True, 1, 4),
     (dict(aa=False, ss=1, gps=False, hybrid=True), True, 0, 2),
     (dict(aa=False, ss=1, gps=False, hybrid=False), False, 0, 1),
+    (dict(aa=False, ss=1, gps=True, hybrid=False), False, 0, 6),
+    (dict(aa=True, ss=2, gps=True, hybrid=False), False, 1, 3),
 ]
 
 
@@ -78,13 +81,13 @@ def test_samples_in_one_call_with_device_frame_counter(cuda_device):
     assert all(torch.equal(a, b) for a, b in zip(got, ref))
 
 
-@pytest.mark.parametrize("change", ["gps", "reuse", "reproject", "zero"])
+@pytest.mark.parametrize("change", ["gps_hybrid", "reuse", "reproject", "zero"])
 def test_samples_in_one_call_rejects_unsupported_settings(change, cuda_device):
     scene = sgs_scenes.make_scene(sgs_scenes.SceneSpec(n=1_000), seed=8)
     tensors = tuple(t.cuda() for t in scene.tensors())
     cam = sgs_scenes.front_camera(64, 48)
     e = torch.empty(0)
-    flags = dict(aa=False, ss=1, gps=change == "gps", hybrid=False)
+    flags = dict(aa=False, ss=1, gps=change == "gps_hybrid", hybrid=change == "gps_hybrid")
     args = list(_args(tensors, cam, flags, (e, e, e, e), 0))
     n = 0 if change == "zero" else 3
     if change == "reuse":
