@@ -69,7 +69,12 @@ __device__ __forceinline__ PointSource shfl_source(const PointSource& s, const u
     return o;
 }
 
+// kHybrid: bins the Gaussians with many points into the queue; kMulti: a.n_samples frames, one
+// framebuffer each (scatter scheduling only). Both are template switches so that the one-sample
+// scatter kernel carries neither the frame loop nor the binning code.
+template <bool kHybrid, bool kMulti>
 __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulateParams a) {
+    static_assert(!(kHybrid && kMulti), "several samples per call use scatter scheduling");
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
     bool active = idx < a.n;
@@ -98,9 +103,9 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     const uint32_t frame0 = frame_rng(a).frame;
     // several samples of one call (scatter scheduling only): the projection once, then each frame's
     // own point draws into its own framebuffer
-    const uint32_t n_frames = a.hybrid ? 1u : a.n_samples;
+    const uint32_t n_frames = kMulti ? a.n_samples : 1u;
     for (uint32_t sm = 0; sm < n_frames; ++sm) {
-        unsigned long long* fb = a.framebuffer + sm * a.fb_stride;
+        unsigned long long* fb = kMulti ? a.framebuffer + sm * a.fb_stride : a.framebuffer;
         // every lane, culled or padding, draws its Poisson sample (accumulate_scatter.cu:104-124)
         uint2 seed = gps_seed(g, frame0 + sm);
         const uint32_t true_count = poisson_count(seed, importance);
@@ -108,7 +113,7 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
         const uint32_t count = min(true_count, cap);
         if (__ballot_sync(kFullMask, act) == 0) continue;
 
-        if (a.hybrid) {
+        if constexpr (kHybrid) {
             // bin Gaussians with many points: one 64-bit atomic per warp reserves entries and chunks
             const bool want = act && count > kBinningPointThreshold;
             const uint32_t ballot = __ballot_sync(kFullMask, want);
@@ -213,7 +218,9 @@ __global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParam
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, const int num_sms, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
     const unsigned grid = (p.n + kBlock - 1) / kBlock;
-    gps_scatter_kernel<<<grid, kBlock, 0, stream>>>(p);
+    if (p.hybrid) gps_scatter_kernel<true, false><<<grid, kBlock, 0, stream>>>(p);
+    else if (p.n_samples > 1) gps_scatter_kernel<false, true><<<grid, kBlock, 0, stream>>>(p);
+    else gps_scatter_kernel<false, false><<<grid, kBlock, 0, stream>>>(p);
     if (p.hybrid) gps_queue_kernel<<<static_cast<unsigned>(num_sms) * kQueueBlocksPerSM, kBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }
