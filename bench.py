@@ -375,8 +375,22 @@ def run_ours(args, world, rank, local) -> dict | None:
         torch.cuda.empty_cache()
     if not args.no_train and args.workload.startswith("batch_6m"):
         line["train_step"] = train_measure(dev)
+    probe = atomic_probe(dev)
+    line["atomics"] = {"probe": probe}
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(scene_cpu, cam, fl, args.cpu_frames, args.workload)
+        line["cpu_baseline"], counts = cpu_baseline(scene_cpu, cam, fl, args.cpu_frames, args.workload)
+        # fragments evaluated (the reference's clipped-AABB count for stochastic transparency, points
+        # for GPS) and atomics issued per sample-frame, counted by the CPU restatement over the
+        # baseline's frames (other frame indices than the timed ones: the same expectation)
+        acc_s = acc_ms * 1e-3
+        line["atomics"].update({
+            "fragments_per_sample_frame": round(counts["fragments"]),
+            "issued_per_sample_frame": round(counts["accepted"]),
+            "fragments_per_s": round(counts["fragments"] / acc_s, 0),
+            "issued_per_s": round(counts["accepted"] / acc_s, 0),
+            "frac_of_probe_rows": round(counts["accepted"] / acc_s / probe["rows_per_s"], 4),
+            "counts_source": f"CPU restatement, mean of {args.cpu_frames} frames; rates over the accumulate stage",
+        })
     return line
 
 
@@ -538,7 +552,7 @@ def batch_graph(scene, fl, dev, steps: int) -> dict:
             "megapixels_per_s_graph": round(pixels / (graph_ms * 1e-3) / 1e6, 1)}
 
 
-def cpu_baseline(scene_cpu, cam, fl, frames: int, workload: str) -> dict:
+def cpu_baseline(scene_cpu, cam, fl, frames: int, workload: str) -> tuple[dict, dict]:
     """The C++ restatement of the reference path (oracle/) on all host cores, a bounded sample."""
     from oracle import cpu
 
@@ -550,14 +564,42 @@ def cpu_baseline(scene_cpu, cam, fl, frames: int, workload: str) -> dict:
               position=cam.position.numpy())
     hist = None
     fb = cpu.accumulate(sc, cd, fl, 0, threads=threads)  # warm-up (page-in, thread pool)
+    counts = {"fragments": 0, "accepted": 0}
     t = time.perf_counter()
     for f in range(frames):
-        fb = cpu.accumulate(sc, cd, fl, f + 1, threads=threads)
+        fb, st = cpu.accumulate(sc, cd, fl, f + 1, threads=threads, return_stats=True)
         out = cpu.sample_resolve(sc, cd, fl, fb, history=hist, temporal_mode=1 if hist else 0, threads=threads)
         hist = (out["image"], out["depth"], out["alpha"], out["weight_mass"])
+        counts["fragments"] += st["fragments"]
+        counts["accepted"] += st["accepted"]
     dt = time.perf_counter() - t
-    return {"value": round(frames / dt, 4), "unit": UNIT, "cores": threads, "kind": "port",
+    line = {"value": round(frames / dt, 4), "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{frames} sample-frames of {workload} (accumulate + sample + resolve), {dt:.1f} s"}
+    per_frame = {k: v / max(frames, 1) for k, v in counts.items()}
+    return line, per_frame
+
+
+def atomic_probe(dev, slots_log2: int = 21, ops: int = 256, launches: int = 5) -> dict:
+    """red.min.u64 reductions per second of the library's probe kernel (sgs_probe_atomic_min) into
+    2^21 u64 slots (16.8 MB, L2-resident like the 1080p framebuffer), 8 blocks of 256 threads per SM,
+    for both access patterns; CUDA events around `launches` launches after two warm-up launches."""
+    from StochasticGSCudaBackend import _C
+
+    slots = torch.full((1 << slots_log2,), -1, dtype=torch.int64, device=dev)
+    blocks = torch.cuda.get_device_properties(dev).multi_processor_count * 8
+    stream = torch.cuda.current_stream(dev)
+    out = {"slots": 1 << slots_log2, "blocks": blocks, "threads_per_block": 256, "ops_per_thread": ops}
+    for name, pattern in (("random", 0), ("rows", 1)):
+        for _ in range(2):
+            _C.probe_atomic_min(slots, ops, blocks, pattern, seed=7)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        t0.record(stream)
+        issued = sum(_C.probe_atomic_min(slots, ops, blocks, pattern, seed=k) for k in range(launches))
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        out[f"{name}_per_s"] = round(issued / (t0.elapsed_time(t1) * 1e-3), 0)
+    return out
 
 
 def run_reference(args, world, rank) -> dict | None:

@@ -306,6 +306,16 @@ void sgs_set_stage_events(void* accumulate_start, void* accumulate_end);
  * place by their warp (same framebuffer); tests use a small cap to exercise that path. */
 void sgs_set_queue_limit(uint32_t max_entries);
 
+/* Measurement aid without a counterpart in the reference: launches `blocks` blocks of 256 threads,
+ * each thread issuing `ops_per_thread` 64-bit atomic minimum reductions (red.min.u64, the merge of
+ * every accumulate pass) into `slots` (n_slots u64 entries, a power of two, 8-byte aligned, device
+ * memory). Pattern 0 spreads the reductions over unrelated slots; pattern 1 lets each thread walk
+ * its own run of consecutive slots, as one lane of the row walker walks a framebuffer row. Time it
+ * with events on `stream`: blocks * 256 * ops_per_thread reductions per launch give the ceiling
+ * against which a render's atomics per second are read. */
+int sgs_probe_atomic_min(void* slots, uint64_t n_slots, uint32_t ops_per_thread, uint32_t blocks, uint32_t pattern,
+                         uint32_t seed, void* stream);
+
 /* Process-wide frame index (render.cu:56-57 keeps it in a hidden static counter that starts at 0);
  * exposed so that random streams can be pinned and resumed. */
 uint32_t sgs_get_frame_index(void);

@@ -78,6 +78,20 @@ def set_queue_limit(max_entries: int = 0) -> None:
     _lib.sgs_set_queue_limit(int(max_entries))
 
 
+def probe_atomic_min(slots: torch.Tensor, ops_per_thread: int, blocks: int, pattern: int = 0, seed: int = 0) -> int:
+    """Launches the red.min.u64 throughput probe (sgs_probe_atomic_min) on the current stream into
+    `slots` (a contiguous int64 CUDA tensor of power-of-two length); returns the number of
+    reductions issued. Measurement aid (no counterpart in the reference module)."""
+    _check(slots.is_cuda and slots.dtype == torch.int64 and slots.is_contiguous(),
+           "slots must be a contiguous int64 CUDA tensor")
+    stream = torch.cuda.current_stream(slots.device).cuda_stream
+    status = _lib.sgs_probe_atomic_min(ctypes.c_void_p(slots.data_ptr()), slots.numel(), int(ops_per_thread),
+                                       int(blocks), int(pattern), int(seed) & 0xFFFFFFFF, ctypes.c_void_p(stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_probe_atomic_min failed ({status}): {_abi.last_error(_lib)}")
+    return int(blocks) * 256 * int(ops_per_thread)
+
+
 def _check(cond: bool, msg: str) -> None:
     if not cond:
         raise RuntimeError(msg)

@@ -172,6 +172,8 @@ SIGNATURES = {
     "sgs_denoise_status": (ctypes.c_int, [ctypes.c_void_p]),
     "sgs_set_stage_events": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_set_queue_limit": (None, [ctypes.c_uint32]),
+    "sgs_probe_atomic_min": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
     "sgs_get_frame_index": (ctypes.c_uint32, []),
     "sgs_set_frame_index": (None, [ctypes.c_uint32]),
     "sgs_k_buffer_size": (ctypes.c_uint32, []),

@@ -394,6 +394,20 @@ int sgs_render_samples(const sgs_gaussians* g, const sgs_camera* c, const sgs_se
 
 void sgs_set_queue_limit(uint32_t max_entries) { g_queue_limit.store(max_entries, std::memory_order_relaxed); }
 
+int sgs_probe_atomic_min(void* slots, uint64_t n_slots, uint32_t ops_per_thread, uint32_t blocks, uint32_t pattern,
+                         uint32_t seed, void* stream) {
+    if (slots == nullptr || (reinterpret_cast<uintptr_t>(slots) & 7u) != 0)
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "slots must be an 8-byte aligned device pointer");
+    if (n_slots == 0 || (n_slots & (n_slots - 1)) != 0)
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "n_slots must be a power of two");
+    if (blocks == 0 || blocks > (1u << 20) || ops_per_thread == 0 || ops_per_thread > (1u << 16) || pattern > 1)
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "blocks 1..2^20, ops_per_thread 1..2^16, pattern 0 or 1");
+    const cudaError_t err = launch_atomic_min_probe(static_cast<unsigned long long*>(slots), n_slots, ops_per_thread,
+                                                    blocks, pattern, seed, static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "atomic probe launch: %s", cudaGetErrorString(err));
+    return SGS_OK;
+}
+
 void sgs_set_stage_events(void* accumulate_start, void* accumulate_end) {
     t_stage_start = static_cast<cudaEvent_t>(accumulate_start);
     t_stage_end = static_cast<cudaEvent_t>(accumulate_end);

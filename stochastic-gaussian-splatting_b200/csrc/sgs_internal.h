@@ -90,6 +90,8 @@ cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue
                          cudaStream_t stream);
 cudaError_t launch_accumulate_st(const AccumulateParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_atomic_min_probe(unsigned long long* slots, uint64_t n_slots, uint32_t ops, uint32_t blocks,
+                                    uint32_t pattern, uint32_t seed, cudaStream_t stream);
 
 struct ResolveParams {
     const float* means;
