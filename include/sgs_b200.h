@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define SGS_ABI_VERSION 2
+#define SGS_ABI_VERSION 3
 #define SGS_K_BUFFER_SIZE 4 /* k-buffer entries per (sub)pixel, resolve.h:9 / render.cu:164 */
 
 enum sgs_status {
@@ -48,6 +48,10 @@ typedef struct sgs_gaussians {
     const float* sh_coefficients; /* (N, B, 3) SH coefficients */
     uint32_t n_gaussians;         /* N (0 renders background) */
     uint32_t sh_bases;            /* B: 1, 4, 9 or 16 (degree 0..3) */
+    const float* preactivated;    /* optional (N, 8) from sgs_preactivate, 16-byte aligned, or NULL; when
+                                   * set, the accumulate pass reads covariance and opacity from it (the
+                                   * same bits) instead of rebuilding them from scales, rotations and
+                                   * opacities. It must match those arrays; nothing checks that. */
 } sgs_gaussians;
 
 /* Pinhole camera in image pixels (render.cu:22-31, render_utils.h:19-30). */
@@ -305,6 +309,14 @@ void sgs_set_stage_events(void* accumulate_start, void* accumulate_end);
  * sizes and renders that follow, process-wide. Gaussians that find the queue full are rendered in
  * place by their warp (same framebuffer); tests use a small cap to exercise that path. */
 void sgs_set_queue_limit(uint32_t max_entries);
+
+/* Preactivated layout (README.md:139-142 of the reference lists it as a possible improvement): writes,
+ * for each Gaussian of `gaussians` (scales, rotations and opacities are read), two float4 into `out`
+ * ((N, 8) floats, 16-byte aligned device memory): the upper triangle of the 3-D covariance
+ * R diag(exp(2 s)) R^T as (c11, c12, c13, c22), (c23, c33), then the opacity sigmoid and 1 when the
+ * quaternion is usable (else 0). Computed once per model and passed as
+ * sgs_gaussians.preactivated, it saves the per-sample rebuild; renders stay bit-identical. */
+int sgs_preactivate(const sgs_gaussians* gaussians, float* out, void* stream);
 
 /* Measurement aid without a counterpart in the reference: launches `blocks` blocks of 256 threads,
  * each thread issuing `ops_per_thread` 64-bit atomic minimum reductions (red.min.u64, the merge of

@@ -78,6 +78,29 @@ def set_queue_limit(max_entries: int = 0) -> None:
     _lib.sgs_set_queue_limit(int(max_entries))
 
 
+def preactivate(scales: torch.Tensor, rotations: torch.Tensor, opacities: torch.Tensor) -> torch.Tensor:
+    """The preactivated layout of these Gaussians (sgs_preactivate): an (N, 8) float32 tensor holding,
+    per Gaussian, the 3-D covariance's upper triangle (c11, c12, c13, c22, c23, c33), the opacity
+    sigmoid and 1 (0 for a degenerate quaternion). Compute it once per model and pass it as
+    `preactivated=` to the render calls; recompute it whenever the parameters change."""
+    device = scales.device
+    scales = _cuda_f32(scales, "scales", device)
+    rotations = _cuda_f32(rotations, "rotations", device)
+    opacities = _cuda_f32(opacities, "opacities", device)
+    n = scales.shape[0]
+    _check(tuple(scales.shape) == (n, 3) and tuple(rotations.shape) == (n, 4) and opacities.numel() == n,
+           "scales (N, 3), rotations (N, 4) and opacities (N) must describe the same Gaussians")
+    out = torch.empty((n, 8), dtype=torch.float32, device=device)
+    g = _abi.Gaussians(None, _ptr(scales), _ptr(rotations), _ptr(opacities), None, n, 1, None)
+    with torch.cuda.device(device):
+        stream = torch.cuda.current_stream(device).cuda_stream
+        status = _lib.sgs_preactivate(ctypes.byref(g), ctypes.c_void_p(out.data_ptr()) if n else None,
+                                      ctypes.c_void_p(stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_preactivate failed ({status}): {_abi.last_error(_lib)}")
+    return out
+
+
 def probe_atomic_min(slots: torch.Tensor, ops_per_thread: int, blocks: int, pattern: int = 0, seed: int = 0) -> int:
     """Launches the red.min.u64 throughput probe (sgs_probe_atomic_min) on the current stream into
     `slots` (a contiguous int64 CUDA tensor of power-of-two length); returns the number of
@@ -111,7 +134,7 @@ def _ptr(t: torch.Tensor | None) -> int | None:
 def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, width, height, focal_x, focal_y,
              center_x, center_y, near_plane, far_plane, proper_antialiasing, supersampling_factor_raw, use_gps,
              hybrid_scheduling, spatial_reuse, blue_noise, k_buffer_primitives, k_buffer_occlusion, history_image,
-             history_depth, history_alpha, history_weight_mass, view_to_previous_view, temporal_mode):
+             history_depth, history_alpha, history_weight_mass, view_to_previous_view, temporal_mode, preactivated=None):
     _check(isinstance(means, torch.Tensor) and means.is_cuda, "means must be a CUDA tensor")
     device = means.device
     means = _cuda_f32(means, "means", device)
@@ -168,7 +191,13 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
     else:
         view_to_previous_view = None
 
-    g = _abi.Gaussians(_ptr(means), _ptr(scales), _ptr(rotations), _ptr(opacities), _ptr(sh_coefficients), n, sh_bases)
+    if preactivated is not None:
+        _check(isinstance(preactivated, torch.Tensor) and preactivated.is_cuda and preactivated.device == device
+               and preactivated.dtype == torch.float32 and tuple(preactivated.shape) == (n, 8)
+               and preactivated.is_contiguous() and preactivated.data_ptr() % 16 == 0,
+               "preactivated must be the contiguous (N, 8) float32 CUDA tensor of preactivate()")
+    g = _abi.Gaussians(_ptr(means), _ptr(scales), _ptr(rotations), _ptr(opacities), _ptr(sh_coefficients), n, sh_bases,
+                       _ptr(preactivated))
     c = _abi.Camera(w2c.data_ptr(), cam_position.data_ptr(), width, height, float(focal_x), float(focal_y),
                     float(center_x), float(center_y), float(near_plane), float(far_plane))
     s = _abi.SettingsC(int(bool(proper_antialiasing)), ss, int(bool(use_gps)), int(bool(hybrid_scheduling)),
@@ -179,12 +208,13 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
         _ptr(history_alpha) if mode else None, _ptr(history_weight_mass) if mode else None,
         _ptr(k_buffer_primitives) if spatial_reuse else None, _ptr(k_buffer_occlusion) if spatial_reuse else None)
     # keep the contiguous copies alive for the duration of the call
-    keep = (means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, blue_noise, view_to_previous_view)
+    keep = (means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, blue_noise, view_to_previous_view,
+            preactivated)
     return device, g, c, s, h, (width, height), keep
 
 
-def _render_impl(args, want_workspace: bool, streams=None):
-    device, g, c, s, h, (width, height), keep = _prepare(*args)
+def _render_impl(args, want_workspace: bool, streams=None, preactivated=None):
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated)
     with torch.cuda.device(device):
         opts = dict(dtype=torch.float32, device=device)
         image = torch.empty((height, width, 3), **opts)
@@ -226,38 +256,41 @@ def _render_impl(args, want_workspace: bool, streams=None):
         return (image, depth, alpha, weight_mass), workspace, layout
 
 
-def render(*args):
-    """`_C.render` with the reference's 29 positional arguments; returns (image, depth, alpha, weight_mass)."""
+def render(*args, preactivated=None):
+    """`_C.render` with the reference's 29 positional arguments; returns (image, depth, alpha, weight_mass).
+    `preactivated` (keyword only, not in the reference): the (N, 8) tensor of `preactivate()` for
+    these Gaussians; the accumulate pass then reads covariance and opacity from it (same bits)."""
     if len(args) != 29:
         raise TypeError(f"render() takes 29 positional arguments ({len(args)} given)")
-    return _render_impl(args, want_workspace=False)
+    return _render_impl(args, want_workspace=False, preactivated=preactivated)
 
 
-def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cuda.Stream, *args):
+def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cuda.Stream, *args, preactivated=None):
     """As `render` (the same 29 arguments after the two streams), with the clear and accumulate passes
     enqueued on `accumulate_stream` and the sample and resolve passes on `resolve_stream` (the C ABI's
     sgs_render_split): a following call can accumulate while this one resolves. The outputs are
     complete on `resolve_stream`; the caller orders its other streams against the two."""
     if len(args) != 29:
         raise TypeError(f"render_split() takes 2 streams and 29 positional arguments ({len(args)} given)")
-    return _render_impl(args, want_workspace=False, streams=(accumulate_stream, resolve_stream))
+    return _render_impl(args, want_workspace=False, streams=(accumulate_stream, resolve_stream),
+                        preactivated=preactivated)
 
 
-def render_samples(n_samples: int, *args):
+def render_samples(n_samples: int, *args, preactivated=None):
     """`n_samples` samples in one call (the C ABI's sgs_render_samples): the same 29 arguments as
     `render`, frames f .. f + n_samples - 1 merged in order (the first in the given temporal mode,
     Reset or Static, the rest Static); returns the final (image, depth, alpha, weight_mass), equal
     bit for bit to `n_samples` `render` calls. No spatial reuse; GPS with scatter scheduling only."""
-    return _render_samples(n_samples, args, want_workspace=False)
+    return _render_samples(n_samples, args, want_workspace=False, preactivated=preactivated)
 
 
-def render_samples_with_workspace(n_samples: int, *args):
+def render_samples_with_workspace(n_samples: int, *args, preactivated=None):
     """As `render_samples`, plus the workspace (its framebuffer section holds the n_samples winner
     framebuffers back to back) and its layout."""
-    return _render_samples(n_samples, args, want_workspace=True)
+    return _render_samples(n_samples, args, want_workspace=True, preactivated=preactivated)
 
 
-def _render_samples(n_samples: int, args, want_workspace: bool):
+def _render_samples(n_samples: int, args, want_workspace: bool, preactivated=None):
     if len(args) != 29:
         raise TypeError(f"render_samples() takes n_samples and 29 render arguments ({len(args)} given)")
     n = int(n_samples)
@@ -265,12 +298,12 @@ def _render_samples(n_samples: int, args, want_workspace: bool):
     device = args[0].device if isinstance(args[0], torch.Tensor) else None
     if device is not None and device.type == "cuda" and device.index != torch.cuda.current_device():
         with torch.cuda.device(device):
-            return _render_samples_impl(n, args, want_workspace)
-    return _render_samples_impl(n, args, want_workspace)
+            return _render_samples_impl(n, args, want_workspace, preactivated)
+    return _render_samples_impl(n, args, want_workspace, preactivated)
 
 
-def _render_samples_impl(n: int, args, want_workspace: bool):
-    device, g, c, s, h, (width, height), keep = _prepare(*args)
+def _render_samples_impl(n: int, args, want_workspace: bool, preactivated=None):
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated)
     _check(not (s.use_gps and s.hybrid_scheduling) and not s.spatial_reuse and s.temporal_mode in (0, 1),
            "render_samples needs no spatial reuse, Reset or Static mode, and for GPS scatter scheduling")
     opts = dict(dtype=torch.float32, device=device)
@@ -304,7 +337,7 @@ def workspace_size(*args) -> int:
     return n
 
 
-def render_into(outputs, workspace: torch.Tensor, streams, *args) -> None:
+def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=None) -> None:
     """Renders like `render` into caller-owned buffers: `outputs` = (image (H, W, 3), depth, alpha,
     weight_mass (H, W, 1)) float32 CUDA tensors, `workspace` a uint8 CUDA tensor of at least
     `workspace_size(*args)` bytes (256-byte aligned), `streams` = None (current stream) or
@@ -312,7 +345,7 @@ def render_into(outputs, workspace: torch.Tensor, streams, *args) -> None:
     be captured in a CUDA graph with fixed buffers (for example ping-ponged histories)."""
     if len(args) != 29:
         raise TypeError(f"render_into() takes outputs, workspace, streams and 29 render arguments ({len(args)} given)")
-    device, g, c, s, h, (width, height), keep = _prepare(*args)
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated)
     shapes = ((height, width, 3), (height, width, 1), (height, width, 1), (height, width, 1))
     for name, t, shape in zip(("image", "depth", "alpha", "weight_mass"), outputs, shapes):
         _check(isinstance(t, torch.Tensor) and t.is_cuda and t.device == device and t.dtype == torch.float32
@@ -336,11 +369,11 @@ def render_into(outputs, workspace: torch.Tensor, streams, *args) -> None:
     del keep
 
 
-def render_with_workspace(*args):
+def render_with_workspace(*args, preactivated=None):
     """As `render`, plus the workspace tensor and its layout (winner framebuffer, samples, reuse weights)."""
     if len(args) != 29:
         raise TypeError(f"render_with_workspace() takes 29 positional arguments ({len(args)} given)")
-    return _render_impl(args, want_workspace=True)
+    return _render_impl(args, want_workspace=True, preactivated=preactivated)
 
 
 def workspace_views(workspace: torch.Tensor, layout, n_fb: int, spatial_reuse: bool) -> dict[str, torch.Tensor]:

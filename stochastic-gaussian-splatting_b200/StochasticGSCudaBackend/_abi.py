@@ -9,7 +9,7 @@ import ctypes
 from pathlib import Path
 
 LIB_NAME = "libsgs_b200.so"
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 SGS_OK = 0
 SGS_ERROR_INVALID_ARGUMENT = -1
@@ -26,6 +26,7 @@ class Gaussians(ctypes.Structure):
         ("sh_coefficients", ctypes.c_void_p),
         ("n_gaussians", ctypes.c_uint32),
         ("sh_bases", ctypes.c_uint32),
+        ("preactivated", ctypes.c_void_p),
     ]
 
 
@@ -172,6 +173,7 @@ SIGNATURES = {
     "sgs_denoise_status": (ctypes.c_int, [ctypes.c_void_p]),
     "sgs_set_stage_events": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_set_queue_limit": (None, [ctypes.c_uint32]),
+    "sgs_preactivate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_probe_atomic_min": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
     "sgs_get_frame_index": (ctypes.c_uint32, []),

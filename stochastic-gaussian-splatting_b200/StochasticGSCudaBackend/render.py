@@ -97,7 +97,12 @@ def render(
     history: History,
     view_to_previous_view: torch.Tensor,
     temporal_mode: TemporalMode,
+    *,
+    preactivated: torch.Tensor | None = None,
 ) -> History:
+    """One sample-frame (render.py:72-96 of the reference). `preactivated` (keyword only, an
+    addition): the `_C.preactivate(scales, rotations, opacities)` tensor of these Gaussians, read by
+    the accumulate pass in place of the per-sample covariance and sigmoid (same bits)."""
     return History(*_C.render(
         means,
         scales,
@@ -110,4 +115,5 @@ def render(
         *history,
         view_to_previous_view,
         int(temporal_mode),
+        preactivated=preactivated,
     ))

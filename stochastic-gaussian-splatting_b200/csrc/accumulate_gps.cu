@@ -27,6 +27,7 @@ constexpr uint32_t kFullMask = 0xffffffffu;
 constexpr uint32_t kBinningPointThreshold = 512;  // accumulate_hybrid_gps.cu:21
 constexpr uint32_t kChunkPoints = 256;             // accumulate_hybrid_gps.cu:19
 constexpr uint32_t kQueueBlocksPerSM = 8;
+constexpr uint32_t kChunksPerClaim = 4;  // chunks a consumer warp takes per atomic on the cursor
 
 struct PointSource {
     float2 mean2d;
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     const uint32_t g = active ? idx : a.n - 1;
 
     Projected p;
-    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p)) return;
+    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre)) return;
 
     // importance and number of points (accumulate_scatter.cu:104-112)
     PointSource s;
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
                 base = __shfl_sync(kFullMask, base, leader);
                 const uint32_t e = static_cast<uint32_t>(base >> kQueueEntryShift) + __popc(ballot & ((1u << lane) - 1u));
                 const unsigned long long first_chunk = (base & kQueueChunkMask) + (incl - chunks);
-                if (want && e < a.max_binned && e < a.q.capacity && first_chunk + chunks <= 0xffffffffull) {
+                if (want && e < a.max_binned && e < a.q.capacity && first_chunk + chunks <= kMaxQueueChunks) {
                     a.q.key[e] = s.key;
                     a.q.geom[e] = make_float4(s.mean2d.x, s.mean2d.y, s.L.x, s.L.y);
                     a.q.geom2[e] = make_float4(s.L.z, s.power_threshold, s.opacity_rcp, s.opacity_dilog);
@@ -167,8 +168,9 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     }
 }
 
-// Persistent consumer of the binned Gaussians: each warp steals one 256-point chunk at a time
-// (accumulate_hybrid_gps.cu:126-181 with per-point counter-based seeds).
+// Persistent consumer of the binned Gaussians: each warp steals kChunksPerClaim 256-point chunks at
+// a time (accumulate_hybrid_gps.cu:126-181 with per-point counter-based seeds, so which warp draws
+// which chunk does not change the winners).
 __global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParams a) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long packed = a.queue->packed;
@@ -178,37 +180,34 @@ __global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParam
     const uint32_t last_first = a.q.meta[n_entries - 1].w;
     const uint32_t n_chunks = last_first + (a.q.count[n_entries - 1] + kChunkPoints - 1) / kChunkPoints;
     for (;;) {
-        uint32_t c = 0;
-        if (lane == 0) c = atomicAdd(&a.queue->next_chunk, 1u);
-        c = __shfl_sync(kFullMask, c, 0);
-        if (c >= n_chunks) break;
-        uint32_t lo = 0, hi = n_entries - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (a.q.meta[mid].w <= c) lo = mid;
-            else hi = mid - 1;
-        }
-        const uint4 m = a.q.meta[lo];
-        const float4 gm = a.q.geom[lo];
-        const float4 gm2 = a.q.geom2[lo];
-        PointSource s;
-        s.key = a.q.key[lo];
-        s.mean2d = make_float2(gm.x, gm.y);
-        s.L = make_float3(gm.z, gm.w, gm2.x);
-        s.power_threshold = gm2.y;
-        s.opacity_rcp = gm2.z;
-        s.opacity_dilog = gm2.w;
-        s.conic = make_float3(__uint_as_float(m.x), __uint_as_float(m.y), __uint_as_float(m.z));
-        const uint32_t n_points = a.q.count[lo];
-        const uint32_t gaussian = static_cast<uint32_t>(s.key);
-        const uint2 base_seed = gps_seed(gaussian, frame_rng(a).frame);
-        const uint32_t first_point = (c - m.w) * kChunkPoints;
-        for (uint32_t k = lane; k < kChunkPoints; k += 32) {
-            const uint32_t point = first_point + k;
-            if (point >= n_points) break;
-            uint2 seed = base_seed;
-            seed.x ^= point * 0x9E3779B9u;
-            gps_point(a, a.framebuffer, seed, s);
+        uint32_t c0 = 0;
+        if (lane == 0) c0 = atomicAdd(&a.queue->next_chunk, kChunksPerClaim);
+        c0 = __shfl_sync(kFullMask, c0, 0);
+        if (c0 >= n_chunks) break;
+        for (uint32_t c = c0; c < min(c0 + kChunksPerClaim, n_chunks); ++c) {
+            const uint32_t lo = queue_entry_of_chunk(a.q.meta, n_entries, c, lane);
+            const uint4 m = a.q.meta[lo];
+            const float4 gm = a.q.geom[lo];
+            const float4 gm2 = a.q.geom2[lo];
+            PointSource s;
+            s.key = a.q.key[lo];
+            s.mean2d = make_float2(gm.x, gm.y);
+            s.L = make_float3(gm.z, gm.w, gm2.x);
+            s.power_threshold = gm2.y;
+            s.opacity_rcp = gm2.z;
+            s.opacity_dilog = gm2.w;
+            s.conic = make_float3(__uint_as_float(m.x), __uint_as_float(m.y), __uint_as_float(m.z));
+            const uint32_t n_points = a.q.count[lo];
+            const uint32_t gaussian = static_cast<uint32_t>(s.key);
+            const uint2 base_seed = gps_seed(gaussian, frame_rng(a).frame);
+            const uint32_t first_point = (c - m.w) * kChunkPoints;
+            for (uint32_t k = lane; k < kChunkPoints; k += 32) {
+                const uint32_t point = first_point + k;
+                if (point >= n_points) break;
+                uint2 seed = base_seed;
+                seed.x ^= point * 0x9E3779B9u;
+                gps_point(a, a.framebuffer, seed, s);
+            }
         }
     }
 }

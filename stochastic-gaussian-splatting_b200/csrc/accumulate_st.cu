@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
     const uint32_t g = active ? idx : a.n - 1;
 
     Projected p;
-    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p)) return;
+    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre)) return;
     const FrameRng rng = frame_rng(a);
 
     const PixelRect rect = pixel_rect(p.bounds, a.cam);
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateP
         const unsigned long long old = atomicAdd(&a.queue->packed, (1ull << kQueueEntryShift) | chunks);
         const uint32_t e = static_cast<uint32_t>(old >> kQueueEntryShift);
         const unsigned long long first_chunk = old & kQueueChunkMask;
-        if (e < a.q.capacity && first_chunk + chunks <= 0xffffffffull) {
+        if (e < a.q.capacity && first_chunk + chunks <= kMaxQueueChunks) {
             a.q.key[e] = key;
             a.q.geom[e] = make_float4(G.mx, G.my, G.cx, G.cy);
             a.q.geom2[e] = make_float4(G.cz, G.opacity, __uint_as_float(rect.x_min), __uint_as_float(rect.width));
@@ -399,13 +399,7 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
         if (lane == 0) c = atomicAdd(&a.queue->next_chunk, 1u);
         c = __shfl_sync(kFullMask, c, 0);
         if (c >= n_chunks) break;
-        // entry owning chunk c: the last one whose first chunk is <= c
-        uint32_t lo = 0, hi = n_entries - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (a.q.meta[mid].w <= c) lo = mid;
-            else hi = mid - 1;
-        }
+        const uint32_t lo = queue_entry_of_chunk(a.q.meta, n_entries, c, lane);
         const uint4 m = a.q.meta[lo];
         const float4 gm = a.q.geom[lo];
         const float4 gm2 = a.q.geom2[lo];

@@ -227,6 +227,8 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
         if (!g->means || !g->scales || !g->rotations || !g->opacities || !g->sh_coefficients)
             return fail(SGS_ERROR_INVALID_ARGUMENT, "null Gaussian array");
         if (!aligned16(g->rotations)) return fail(SGS_ERROR_INVALID_ARGUMENT, "rotations must be 16-byte aligned");
+        if (!aligned16(g->preactivated))
+            return fail(SGS_ERROR_INVALID_ARGUMENT, "the preactivated layout must be 16-byte aligned");
     }
     if (g->sh_bases != 1 && g->sh_bases != 4 && g->sh_bases != 9 && g->sh_bases != 16)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "sh_bases must be 1, 4, 9 or 16 (got %u)", g->sh_bases);
@@ -298,6 +300,7 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
         ap.q = w.q;
         ap.n_samples = n_samples;
         ap.fb_stride = d.n_fb;
+        ap.pre = reinterpret_cast<const float4*>(g->preactivated);
         if (t_stage_start != nullptr) cudaEventRecord(t_stage_start, stream);
         err = s->use_gps ? launch_accumulate_gps(ap, sms, stream) : launch_accumulate_st(ap, sms, stream);
         if (t_stage_end != nullptr && err == cudaSuccess) err = cudaEventRecord(t_stage_end, stream);
@@ -393,6 +396,20 @@ int sgs_render_samples(const sgs_gaussians* g, const sgs_camera* c, const sgs_se
 }
 
 void sgs_set_queue_limit(uint32_t max_entries) { g_queue_limit.store(max_entries, std::memory_order_relaxed); }
+
+int sgs_preactivate(const sgs_gaussians* g, float* out, void* stream) {
+    if (g == nullptr) return fail(SGS_ERROR_INVALID_ARGUMENT, "null argument");
+    if (g->n_gaussians == 0) return SGS_OK;
+    if (out == nullptr) return fail(SGS_ERROR_INVALID_ARGUMENT, "null output");
+    if (!g->scales || !g->rotations || !g->opacities) return fail(SGS_ERROR_INVALID_ARGUMENT, "null Gaussian array");
+    if (!aligned16(g->rotations) || !aligned16(out))
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "rotations and the output must be 16-byte aligned");
+    const cudaError_t err = launch_preactivate(g->scales, reinterpret_cast<const float4*>(g->rotations), g->opacities,
+                                               g->n_gaussians, reinterpret_cast<float4*>(out),
+                                               static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "preactivate launch: %s", cudaGetErrorString(err));
+    return SGS_OK;
+}
 
 int sgs_probe_atomic_min(void* slots, uint64_t n_slots, uint32_t ops_per_thread, uint32_t blocks, uint32_t pattern,
                          uint32_t seed, void* stream) {

@@ -21,6 +21,9 @@ struct WorkQueue {
 };
 constexpr unsigned long long kQueueEntryShift = 40;
 constexpr unsigned long long kQueueChunkMask = (1ull << kQueueEntryShift) - 1;
+// Producers queue chunk indices below this, so the consumers' cursor (which overshoots the last chunk
+// by at most one claim per warp) cannot wrap around.
+constexpr unsigned long long kMaxQueueChunks = 0xffffffffull - (1ull << 24);
 
 // Per-entry arrays of the large-Gaussian queue (structure of arrays, 16-byte aligned).
 struct QueueArrays {
@@ -31,6 +34,25 @@ struct QueueArrays {
     uint32_t* count;          // GPS: number of points
     uint32_t capacity;
 };
+
+// Queue entry owning chunk c: the last e in [0, n) with meta[e].w (the entry's first chunk,
+// nondecreasing in e, meta[0].w = 0) <= c. A 32-ary search by the whole warp (every lane calls it
+// with the same arguments): each step the lanes read 32 evenly spaced first chunks at once and a
+// ballot keeps the segment that holds the answer, so 2^20 entries take 4 rounds of loads instead
+// of 20 dependent ones.
+__device__ __forceinline__ uint32_t queue_entry_of_chunk(const uint4* __restrict__ meta, const uint32_t n,
+                                                         const uint32_t c, const uint32_t lane) {
+    uint32_t lo = 0, hi = n;  // the answer lies in [lo, hi)
+    while (hi - lo > 1u) {
+        const uint32_t step = (hi - lo + 31u) >> 5;
+        const uint32_t idx = lo + lane * step;
+        const bool le = lane == 0u || (idx < hi && meta[idx].w <= c);
+        const uint32_t k = 31u - __clz(__ballot_sync(0xffffffffu, le));
+        lo += k * step;
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
 
 // Scratch carved out of the caller's workspace by layout_workspace().
 struct Workspace {
@@ -61,6 +83,7 @@ struct AccumulateParams {
     QueueArrays q;
     uint32_t n_samples;               // samples of one call (frames frame .. frame + n_samples - 1)
     size_t fb_stride;                 // framebuffer elements between consecutive samples' framebuffers
+    const float4* pre;                // preactivated layout (2 float4 per Gaussian) or null
 };
 
 // Frame-dependent random-number state of one call: the frame index (from device memory when the
@@ -90,6 +113,8 @@ cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue
                          cudaStream_t stream);
 cudaError_t launch_accumulate_st(const AccumulateParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_preactivate(const float* scales, const float4* rotations, const float* opacities, uint32_t n,
+                              float4* out, cudaStream_t stream);
 cudaError_t launch_atomic_min_probe(unsigned long long* slots, uint64_t n_slots, uint32_t ops, uint32_t blocks,
                                     uint32_t pattern, uint32_t seed, cudaStream_t stream);
 

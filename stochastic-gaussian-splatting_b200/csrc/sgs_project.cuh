@@ -34,24 +34,15 @@ struct Projected {
     float4 bounds;  // x_min, x_max, y_min, y_max in (sub)pixels
 };
 
-// Loads and projects Gaussian `g`; clears `active` when it is culled. Returns false when no lane
-// of the calling warp is active after the depth test or at the end (the warp may then skip the
-// rest of its work); the early exits mirror gs_utils.h:74-75,189-190 and keep the loads of culled
-// warps from happening.
-__device__ __forceinline__ bool project_gaussian(bool& active, const uint32_t g, const float* __restrict__ means,
-                                                 const float* __restrict__ scales, const float4* __restrict__ rotations,
-                                                 const float* __restrict__ opacities, const float4* __restrict__ w2c,
-                                                 const PassCamera& cam, Projected& p) {
-    const float mx = means[3 * g + 0], my = means[3 * g + 1], mz = means[3 * g + 2];
-    const float4 r3 = w2c[2];
-    p.depth = r3.x * mx + r3.y * my + r3.z * mz + r3.w;
-    if (p.depth < cam.near_plane || p.depth > cam.far_plane) active = false;
-    if (__ballot_sync(0xffffffffu, active) == 0) return false;
+// Upper triangle of the 3-D covariance R diag(exp(2 s)) R^T of Gaussian g (gs_utils.h:82-110);
+// clears `valid` for a degenerate quaternion. The projection and the preactivated layout both take
+// it from here, so the two hold the same bits.
+struct Cov3d {
+    float c11, c12, c13, c22, c23, c33;
+};
 
-    const float raw_opacity = opacities[g];
-    p.opacity = 1.0f / (1.0f + expf(-raw_opacity));
-    if (p.opacity < kMinAlpha) active = false;
-
+__device__ __forceinline__ Cov3d cov3d_of(const uint32_t g, const float* __restrict__ scales,
+                                          const float4* __restrict__ rotations, bool& valid) {
     const float vx = expf(2.0f * scales[3 * g + 0]);
     const float vy = expf(2.0f * scales[3 * g + 1]);
     const float vz = expf(2.0f * scales[3 * g + 2]);
@@ -61,7 +52,7 @@ __device__ __forceinline__ bool project_gaussian(bool& active, const uint32_t g,
     const float ij = i * j, ik = i * k, jk = j * k;
     const float ri = r * i, rj = r * j, rk = r * k;
     const float norm_sq = r * r + ii + jj + kk;
-    if (norm_sq < 1e-8f) active = false;
+    if (norm_sq < 1e-8f) valid = false;
     const float n_rcp = 1.0f / norm_sq;
     const float R11 = 1.0f - 2.0f * (jj + kk) * n_rcp, R12 = 2.0f * (ij - rk) * n_rcp, R13 = 2.0f * (ik + rj) * n_rcp;
     const float R21 = 2.0f * (ij + rk) * n_rcp, R22 = 1.0f - 2.0f * (ii + kk) * n_rcp, R23 = 2.0f * (jk - ri) * n_rcp;
@@ -69,13 +60,60 @@ __device__ __forceinline__ bool project_gaussian(bool& active, const uint32_t g,
     const float S11 = R11 * vx, S12 = R12 * vy, S13 = R13 * vz;
     const float S21 = R21 * vx, S22 = R22 * vy, S23 = R23 * vz;
     const float S31 = R31 * vx, S32 = R32 * vy, S33 = R33 * vz;
-    // upper triangle of R diag(v) R^T
-    const float c11 = S11 * R11 + S12 * R12 + S13 * R13;
-    const float c12 = S11 * R21 + S12 * R22 + S13 * R23;
-    const float c13 = S11 * R31 + S12 * R32 + S13 * R33;
-    const float c22 = S21 * R21 + S22 * R22 + S23 * R23;
-    const float c23 = S21 * R31 + S22 * R32 + S23 * R33;
-    const float c33 = S31 * R31 + S32 * R32 + S33 * R33;
+    Cov3d c;
+    c.c11 = S11 * R11 + S12 * R12 + S13 * R13;
+    c.c12 = S11 * R21 + S12 * R22 + S13 * R23;
+    c.c13 = S11 * R31 + S12 * R32 + S13 * R33;
+    c.c22 = S21 * R21 + S22 * R22 + S23 * R23;
+    c.c23 = S21 * R31 + S22 * R32 + S23 * R33;
+    c.c33 = S31 * R31 + S32 * R32 + S33 * R33;
+    return c;
+}
+
+// Sigmoid of the opacity logit (gs_utils.h:77-79).
+__device__ __forceinline__ float opacity_of(const float raw_opacity) { return 1.0f / (1.0f + expf(-raw_opacity)); }
+
+// Preactivated layout of one Gaussian: two float4, (c11, c12, c13, c22) and (c23, c33, opacity,
+// 1 when the quaternion is usable else 0), computed once by sgs_preactivate from the same code.
+__device__ __forceinline__ void preactivated_of(const uint32_t g, const float* __restrict__ scales,
+                                                const float4* __restrict__ rotations,
+                                                const float* __restrict__ opacities, float4& v0, float4& v1) {
+    bool valid = true;
+    const Cov3d c = cov3d_of(g, scales, rotations, valid);
+    v0 = make_float4(c.c11, c.c12, c.c13, c.c22);
+    v1 = make_float4(c.c23, c.c33, opacity_of(opacities[g]), valid ? 1.0f : 0.0f);
+}
+
+// Loads and projects Gaussian `g`; clears `active` when it is culled. Returns false when no lane
+// of the calling warp is active after the depth test or at the end (the warp may then skip the
+// rest of its work); the early exits mirror gs_utils.h:74-75,189-190 and keep the loads of culled
+// warps from happening.
+// `pre` (nullable): the preactivated layout of the same Gaussians; when given, covariance and
+// opacity are read from it instead of being rebuilt from scales, rotations and the opacity logit.
+__device__ __forceinline__ bool project_gaussian(bool& active, const uint32_t g, const float* __restrict__ means,
+                                                 const float* __restrict__ scales, const float4* __restrict__ rotations,
+                                                 const float* __restrict__ opacities, const float4* __restrict__ w2c,
+                                                 const PassCamera& cam, Projected& p,
+                                                 const float4* __restrict__ pre = nullptr) {
+    const float mx = means[3 * g + 0], my = means[3 * g + 1], mz = means[3 * g + 2];
+    const float4 r3 = w2c[2];
+    p.depth = r3.x * mx + r3.y * my + r3.z * mz + r3.w;
+    if (p.depth < cam.near_plane || p.depth > cam.far_plane) active = false;
+    if (__ballot_sync(0xffffffffu, active) == 0) return false;
+
+    Cov3d cv;
+    if (pre != nullptr) {
+        const float4 v0 = pre[2 * g], v1 = pre[2 * g + 1];
+        p.opacity = v1.z;
+        if (p.opacity < kMinAlpha) active = false;
+        if (v1.w == 0.0f) active = false;
+        cv.c11 = v0.x, cv.c12 = v0.y, cv.c13 = v0.z, cv.c22 = v0.w, cv.c23 = v1.x, cv.c33 = v1.y;
+    } else {
+        p.opacity = opacity_of(opacities[g]);
+        if (p.opacity < kMinAlpha) active = false;
+        cv = cov3d_of(g, scales, rotations, active);
+    }
+    const float c11 = cv.c11, c12 = cv.c12, c13 = cv.c13, c22 = cv.c22, c23 = cv.c23, c33 = cv.c33;
 
     const float4 r1 = w2c[0];
     const float x = (r1.x * mx + r1.y * my + r1.z * mz + r1.w) / p.depth;

@@ -81,8 +81,10 @@ class ProgressiveRenderer:
     def __init__(self, means, scales, rotations, opacities, sh_coefficients, *, proper_antialiasing: bool = False,
                  use_gps: bool = False, hybrid_scheduling: bool = False, supersampling_factor: int = 1,
                  samples_per_pixel: int = 1, disable_progressive_rendering: bool = False,
-                 spatial_reuse: bool = False, temporal_reuse: bool = False):
+                 spatial_reuse: bool = False, temporal_reuse: bool = False, preactivate: bool = False):
         self.model = (means, scales, rotations, opacities, sh_coefficients)
+        # covariance and opacity sigmoid once per model (README.md:139-142); the images are the same bits
+        self.preactivated = _C.preactivate(scales, rotations, opacities) if preactivate else None
         self.device = means.device
         self.proper_antialiasing = proper_antialiasing
         self.use_gps = use_gps
@@ -116,10 +118,11 @@ class ProgressiveRenderer:
         if one_call:
             self.history = History(*_C.render_samples(
                 n, *self.model, *settings.as_tuple(), _blue_noise(self.device), *self.k_buffer, *self.history, v2pv,
-                int(mode)))
+                int(mode), preactivated=self.preactivated))
             return
         for _ in range(n):
-            self.history = render(*self.model, settings, self.k_buffer, self.history, v2pv, mode)
+            self.history = render(*self.model, settings, self.k_buffer, self.history, v2pv, mode,
+                                  preactivated=self.preactivated)
             mode = TemporalMode.STATIC
 
     @torch.inference_mode()

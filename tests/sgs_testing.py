@@ -6,12 +6,14 @@ import torch
 
 
 def render_once(scene: dict, cam: dict, flags: dict, frame_idx: int, *, blue_noise=None, temporal_mode: int = 0,
-                history=None, k_buffer=None, v2pv=None, spatial_reuse: bool = False, device="cuda") -> dict:
+                history=None, k_buffer=None, v2pv=None, spatial_reuse: bool = False, device="cuda",
+                preactivate: bool = False) -> dict:
     """Renders one sample-frame through `_C.render_with_workspace` with the frame index pinned.
 
     `scene` holds numpy or torch arrays (means, scales, rotations, opacities, sh_coefficients), `cam` the
     camera dict of the golden manifest, `flags` aa/ss/gps/hybrid. Returns numpy copies of the winner
     framebuffer, the samples (and reuse weights), the four outputs and the torch outputs for chaining.
+    `preactivate` renders with the preactivated layout of the same Gaussians.
     """
     from StochasticGSCudaBackend import _C
 
@@ -38,7 +40,8 @@ def render_once(scene: dict, cam: dict, flags: dict, frame_idx: int, *, blue_noi
     outs, ws, layout = _C.render_with_workspace(
         *tensors, w2c, pos, cam["width"], cam["height"], cam["focal_x"], cam["focal_y"], cam["center_x"],
         cam["center_y"], cam["near_plane"], cam["far_plane"], flags["aa"], ss, flags["gps"], flags["hybrid"],
-        spatial_reuse, bn, k_buffer[0], k_buffer[1], *history, t(v2pv), temporal_mode)
+        spatial_reuse, bn, k_buffer[0], k_buffer[1], *history, t(v2pv), temporal_mode,
+        preactivated=_C.preactivate(tensors[1], tensors[2], tensors[3]) if preactivate else None)
     views = _C.workspace_views(ws, layout, n_fb, spatial_reuse)
     torch.cuda.synchronize()
     res = {

@@ -132,9 +132,13 @@ def test_python_module_mirrors_the_reference_binding():
                                 "use_gps", "hybrid_scheduling", "spatial_reuse")
     assert [m.name for m in TemporalMode] == ["RESET", "STATIC", "REPROJECT"] and int(TemporalMode.REPROJECT) == 2
     assert History._fields == ("image", "depth", "alpha", "weight_mass")
-    assert list(inspect.signature(render).parameters) == ["means", "scales", "rotations", "opacities",
-                                                          "sh_coefficients", "settings", "k_buffer", "history",
-                                                          "view_to_previous_view", "temporal_mode"]
+    params = inspect.signature(render).parameters.values()
+    positional = [p.name for p in params if p.kind is not inspect.Parameter.KEYWORD_ONLY]
+    assert positional == ["means", "scales", "rotations", "opacities", "sh_coefficients", "settings", "k_buffer",
+                          "history", "view_to_previous_view", "temporal_mode"]
+    # additions are keyword-only with defaults, so every reference call binds unchanged
+    extras = [p for p in params if p.kind is inspect.Parameter.KEYWORD_ONLY]
+    assert [p.name for p in extras] == ["preactivated"] and all(p.default is None for p in extras)
     assert callable(create_k_buffer)
     with pytest.raises(TypeError):
         _C.render(1, 2, 3)

@@ -1,6 +1,7 @@
 """The progressive renderer (sgs_viewer) against the frame logic of Renderer.py:48-103 written as a
 loop of single-sample `render()` calls (GPU): same images, depths and alphas bit for bit, through
-RESET, STATIC, REPROJECT and setting changes; the camera-path benchmark and the PNG output run."""
+RESET, STATIC, REPROJECT and setting changes (also with the preactivated layout on the renderer side
+only); the camera-path benchmark and the PNG output run."""
 import numpy as np
 import pytest
 import torch
@@ -57,7 +58,8 @@ def _views(sgs_viewer):
 
 @pytest.mark.parametrize("flags", [dict(), dict(temporal_reuse=True), dict(temporal_reuse=True, spatial_reuse=True),
                                    dict(supersampling_factor=2, hybrid_scheduling=True),
-                                   dict(use_gps=True, temporal_reuse=True)])
+                                   dict(use_gps=True, temporal_reuse=True), dict(preactivate=True),
+                                   dict(use_gps=True, temporal_reuse=True, spatial_reuse=True, preactivate=True)])
 @pytest.mark.parametrize("spp", [1, 4])
 def test_progressive_renderer_equals_the_sample_loop(flags, spp, cuda_device):
     import sgs_viewer
