@@ -27,7 +27,7 @@ constexpr uint32_t kFullMask = 0xffffffffu;
 constexpr uint32_t kBinningPointThreshold = 512;  // accumulate_hybrid_gps.cu:21
 constexpr uint32_t kChunkPoints = 256;             // accumulate_hybrid_gps.cu:19
 constexpr uint32_t kQueueBlocksPerSM = 8;
-constexpr uint32_t kChunksPerClaim = 4;  // chunks a consumer warp takes per atomic on the cursor
+constexpr uint32_t kChunksPerClaim = 8;  // chunks a consumer warp takes per atomic on the cursor
 
 struct PointSource {
     float2 mean2d;
@@ -39,7 +39,11 @@ struct PointSource {
     unsigned long long key;
 };
 
-// Draws one point from `seed` and merges it (scatter_utils.cuh:116-129).
+// Draws one point from `seed` and merges it (scatter_utils.cuh:116-129). kFilter first reads the
+// pixel's current key (a relaxed load at GPU scope) and skips the atomic when that key is already
+// <= the point's: keys only decrease during a pass, so such a point cannot change the minimum, and
+// the framebuffer ends with the same bits while the L2 atomic units see far fewer operations.
+template <bool kFilter = false>
 __device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned long long* __restrict__ fb, uint2& seed,
                                           const PointSource& s) {
     const float2 u = pcg2d_uniform(seed);
@@ -53,7 +57,13 @@ __device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned lo
     if (power > s.power_threshold) return;
     const uint32_t px = __float2uint_rd(sx);
     const uint32_t py = __float2uint_rd(sy);
-    atomicMin(&fb[py * a.cam.width_int + px], s.key);
+    unsigned long long* const pixel = &fb[py * a.cam.width_int + px];
+    if constexpr (kFilter) {
+        unsigned long long current;
+        asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(current) : "l"(pixel));
+        if (current <= s.key) return;
+    }
+    atomicMin(pixel, s.key);
 }
 
 __device__ __forceinline__ PointSource shfl_source(const PointSource& s, const uint32_t src) {
@@ -171,7 +181,7 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
 // Persistent consumer of the binned Gaussians: each warp steals kChunksPerClaim 256-point chunks at
 // a time (accumulate_hybrid_gps.cu:126-181 with per-point counter-based seeds, so which warp draws
 // which chunk does not change the winners).
-__global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParams a) {
+__global__ void __launch_bounds__(kBlock, kQueueBlocksPerSM) gps_queue_kernel(const AccumulateParams a) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long packed = a.queue->packed;
     const uint32_t cap = min(a.max_binned, a.q.capacity);
@@ -179,34 +189,44 @@ __global__ void __launch_bounds__(kBlock) gps_queue_kernel(const AccumulateParam
     if (n_entries == 0) return;
     const uint32_t last_first = a.q.meta[n_entries - 1].w;
     const uint32_t n_chunks = last_first + (a.q.count[n_entries - 1] + kChunkPoints - 1) / kChunkPoints;
+    const uint32_t frame = frame_rng(a).frame;
     for (;;) {
         uint32_t c0 = 0;
         if (lane == 0) c0 = atomicAdd(&a.queue->next_chunk, kChunksPerClaim);
         c0 = __shfl_sync(kFullMask, c0, 0);
         if (c0 >= n_chunks) break;
-        for (uint32_t c = c0; c < min(c0 + kChunksPerClaim, n_chunks); ++c) {
-            const uint32_t lo = queue_entry_of_chunk(a.q.meta, n_entries, c, lane);
-            const uint4 m = a.q.meta[lo];
-            const float4 gm = a.q.geom[lo];
-            const float4 gm2 = a.q.geom2[lo];
-            PointSource s;
-            s.key = a.q.key[lo];
-            s.mean2d = make_float2(gm.x, gm.y);
-            s.L = make_float3(gm.z, gm.w, gm2.x);
-            s.power_threshold = gm2.y;
-            s.opacity_rcp = gm2.z;
-            s.opacity_dilog = gm2.w;
-            s.conic = make_float3(__uint_as_float(m.x), __uint_as_float(m.y), __uint_as_float(m.z));
-            const uint32_t n_points = a.q.count[lo];
-            const uint32_t gaussian = static_cast<uint32_t>(s.key);
-            const uint2 base_seed = gps_seed(gaussian, frame_rng(a).frame);
-            const uint32_t first_point = (c - m.w) * kChunkPoints;
+        const uint32_t c_end = min(c0 + kChunksPerClaim, n_chunks);
+        // consecutive chunks of a claim mostly belong to one entry: search and load it only when a
+        // chunk lies past the current entry's last chunk
+        uint32_t entry_first = 0, entry_end = 0;
+        PointSource s;
+        uint32_t n_points = 0;
+        uint2 base_seed = make_uint2(0u, 0u);
+        for (uint32_t c = c0; c < c_end; ++c) {
+            if (c >= entry_end) {
+                const uint32_t lo = queue_entry_of_chunk(a.q.meta, n_entries, c, lane);
+                const uint4 m = a.q.meta[lo];
+                const float4 gm = a.q.geom[lo];
+                const float4 gm2 = a.q.geom2[lo];
+                s.key = a.q.key[lo];
+                s.mean2d = make_float2(gm.x, gm.y);
+                s.L = make_float3(gm.z, gm.w, gm2.x);
+                s.power_threshold = gm2.y;
+                s.opacity_rcp = gm2.z;
+                s.opacity_dilog = gm2.w;
+                s.conic = make_float3(__uint_as_float(m.x), __uint_as_float(m.y), __uint_as_float(m.z));
+                n_points = a.q.count[lo];
+                entry_first = m.w;
+                entry_end = m.w + (n_points + kChunkPoints - 1) / kChunkPoints;
+                base_seed = gps_seed(static_cast<uint32_t>(s.key), frame);
+            }
+            const uint32_t first_point = (c - entry_first) * kChunkPoints;
             for (uint32_t k = lane; k < kChunkPoints; k += 32) {
                 const uint32_t point = first_point + k;
                 if (point >= n_points) break;
                 uint2 seed = base_seed;
                 seed.x ^= point * 0x9E3779B9u;
-                gps_point(a, a.framebuffer, seed, s);
+                gps_point<true>(a, a.framebuffer, seed, s);
             }
         }
     }
