@@ -27,6 +27,7 @@ constexpr uint32_t kFullMask = 0xffffffffu;
 constexpr uint32_t kBinningPointThreshold = 512;  // accumulate_hybrid_gps.cu:21
 constexpr uint32_t kChunkPoints = 256;             // accumulate_hybrid_gps.cu:19
 constexpr uint32_t kQueueBlocksPerSM = 8;
+constexpr uint32_t kItemsPerWarp = 128;  // parked cooperative points per warp (multiple of 32)
 constexpr uint32_t kChunksPerClaim = 8;  // chunks a consumer warp takes per atomic on the cursor
 
 struct PointSource {
@@ -39,14 +40,14 @@ struct PointSource {
     unsigned long long key;
 };
 
-// Draws one point from `seed` and merges it (scatter_utils.cuh:116-129). kFilter first reads the
+// Merges the point drawn from uniforms `u` (scatter_utils.cuh:116-129; gps_point draws them from
+// `seed` first). kFilter first reads the
 // pixel's current key (a relaxed load at GPU scope) and skips the atomic when that key is already
 // <= the point's: keys only decrease during a pass, so such a point cannot change the minimum, and
 // the framebuffer ends with the same bits while the L2 atomic units see far fewer operations.
 template <bool kFilter = false>
-__device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned long long* __restrict__ fb, uint2& seed,
-                                          const PointSource& s) {
-    const float2 u = pcg2d_uniform(seed);
+__device__ __forceinline__ void gps_point_at(const AccumulateParams& a, unsigned long long* __restrict__ fb,
+                                             const float2 u, const PointSource& s) {
     const float2 xy = truncated_box_muller(u.x, u.y, s.opacity_rcp, s.opacity_dilog);
     const float sx = s.mean2d.x + s.L.x * xy.x;
     const float sy = s.mean2d.y + (s.L.y * xy.x + s.L.z * xy.y);
@@ -66,6 +67,12 @@ __device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned lo
     atomicMin(pixel, s.key);
 }
 
+template <bool kFilter = false>
+__device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned long long* __restrict__ fb, uint2& seed,
+                                          const PointSource& s) {
+    gps_point_at<kFilter>(a, fb, pcg2d_uniform(seed), s);
+}
+
 __device__ __forceinline__ PointSource shfl_source(const PointSource& s, const uint32_t src) {
     PointSource o;
     o.mean2d = make_float2(__shfl_sync(kFullMask, s.mean2d.x, src), __shfl_sync(kFullMask, s.mean2d.y, src));
@@ -80,13 +87,33 @@ __device__ __forceinline__ PointSource shfl_source(const PointSource& s, const u
     return o;
 }
 
+// Evaluates the n parked points of the warp's cooperative phase, 32 at a time: buffer item b holds
+// the stepped stream state of its point and the lane whose Gaussian it belongs to.
+__device__ __forceinline__ void evaluate_parked(const AccumulateParams& a, unsigned long long* __restrict__ fb,
+                                                const PointSource& s, const uint2* __restrict__ states,
+                                                const uint8_t* __restrict__ srcs, const uint32_t n,
+                                                const uint32_t lane) {
+    __syncwarp();
+    for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t b = base + lane;
+        const bool valid = b < n;
+        const uint32_t src = valid ? srcs[b] : lane;
+        const PointSource t = shfl_source(s, src);
+        if (valid) gps_point_at(a, fb, pcg2d_to_uniform(states[b]), t);
+    }
+    __syncwarp();
+}
+
 // kHybrid: bins the Gaussians with many points into the queue; kMulti: a.n_samples frames, one
 // framebuffer each (scatter scheduling only). Both are template switches so that the one-sample
 // scatter kernel carries neither the frame loop nor the binning code.
 template <bool kHybrid, bool kMulti>
 __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulateParams a) {
     static_assert(!(kHybrid && kMulti), "several samples per call use scatter scheduling");
+    __shared__ uint2 s_state[kBlock / 32][kItemsPerWarp];
+    __shared__ uint8_t s_src[kBlock / 32][kItemsPerWarp];
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
     const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
     bool active = idx < a.n;
     const uint32_t g = active ? idx : a.n - 1;
@@ -160,21 +187,37 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
         // own first points, sequentially per lane
         for (uint32_t i = 0; act && i < count && i < kSequentialFragments; ++i) gps_point(a, fb, seed, s);
 
-        // the rest cooperatively, one large Gaussian at a time in lane order, each lane on its own seed
-        const uint32_t coop = __ballot_sync(kFullMask, act && count > kSequentialFragments);
-        uint32_t pending = coop;
+        // The rest cooperatively, the warp's larger Gaussians in lane order: point j (after the first
+        // kSequentialFragments) of Gaussian src is drawn by lane j % 32 from its own stream, in (src, j)
+        // order (scatter_utils.cuh:140-183). Whole rows of 32 points are evaluated as they are drawn;
+        // the last partial row (fewer than 32 points, most of a short Gaussian's) is drawn in order but
+        // parked in the warp's buffer, and full buffers are evaluated 32 points at a time whatever
+        // Gaussian they belong to, so short Gaussians no longer leave most lanes idle.
+        uint32_t pending = __ballot_sync(kFullMask, act && count > kSequentialFragments);
+        uint32_t fill = 0;
         while (pending) {
             const uint32_t src = __ffs(pending) - 1;
             pending &= pending - 1;
-            const uint32_t n_src = __shfl_sync(kFullMask, count, src);
-            const PointSource t = shfl_source(s, src);
-            const uint32_t iterations = (n_src - kSequentialFragments + 31) / 32;
-            for (uint32_t it = 0; it < iterations; ++it) {
-                const uint32_t fi = it * 32 + lane + kSequentialFragments;
-                if (fi >= n_src) continue;
-                gps_point(a, fb, seed, t);
+            const uint32_t n_items = __shfl_sync(kFullMask, count, src) - kSequentialFragments;
+            const uint32_t full = n_items & ~31u;
+            if (full != 0) {
+                const PointSource t = shfl_source(s, src);
+                for (uint32_t j = lane; j < full; j += 32) gps_point(a, fb, seed, t);
             }
+            const uint32_t rest = n_items - full;
+            if (rest == 0) continue;
+            if (fill + rest > kItemsPerWarp) {
+                evaluate_parked(a, fb, s, s_state[warp], s_src[warp], fill, lane);
+                fill = 0;
+            }
+            if (lane < rest) {
+                pcg2d_step(seed);
+                s_state[warp][fill + lane] = seed;
+                s_src[warp][fill + lane] = static_cast<uint8_t>(src);
+            }
+            fill += rest;
         }
+        if (fill != 0) evaluate_parked(a, fb, s, s_state[warp], s_src[warp], fill, lane);
     }
 }
 

@@ -93,9 +93,14 @@ __device__ __forceinline__ void pcg2d_step(uint2& s) {
     s.y ^= s.y >> 16u;
 }
 
+// The two uniforms in [0, 1) of a stepped PCG2D state.
+__device__ __forceinline__ float2 pcg2d_to_uniform(const uint2 s) {
+    return make_float2(static_cast<float>(s.x) * 2.3283064365387e-10f, static_cast<float>(s.y) * 2.3283064365387e-10f);
+}
+
 __device__ __forceinline__ float2 pcg2d_uniform(uint2& s) {
     pcg2d_step(s);
-    return make_float2(static_cast<float>(s.x) * 2.3283064365387e-10f, static_cast<float>(s.y) * 2.3283064365387e-10f);
+    return pcg2d_to_uniform(s);
 }
 
 // Polynomial approximations of the dilogarithm-based radial CDF used by GPS to draw points
