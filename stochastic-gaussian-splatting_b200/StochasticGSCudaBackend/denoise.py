@@ -1,7 +1,7 @@
 """Learned resolve: a small convolutional denoiser that maps a few samples to the converged image.
 
 The reference resolves only by progressive averaging (resolve.cu, Static mode), which stays the
-fallback and the judge. This module adds, on the same render path:
+fallback and the yardstick its output is measured against. This module adds, on the same render path:
 
 * `render_features(...)`: renders n samples (Reset mode, one frame index each) and builds the
   8-channel FP16 input per pixel: mean premultiplied rgb, mean alpha, mean depth x depth_scale,

@@ -1,7 +1,7 @@
 // Learned resolve: a 6-layer 3x3 convolutional denoiser on BF16 tensor cores (tcgen05, FP32 in TMEM).
 //
 // The reference has no learned resolve; plain progressive averaging (resolve.cu, Static mode) is the
-// fallback and the judge of its error. This file holds every kernel of the denoiser:
+// fallback and the yardstick of its error. This file holds every kernel of the denoiser:
 //   conv3x3_kernel        implicit-GEMM 3x3 convolution, zero padding 1, stride 1. Forward layers
 //                         (bias + ReLU, or bias + residual for the last layer) and data gradients
 //                         (flipped, transposed weights; the ReLU mask of the layer below fused).

@@ -11,7 +11,7 @@ plus the per-Gaussian projection dump of gs_utils.h:38-193.
 
 Inputs are stored beside the outputs (scene_<name>.npz) so the fixtures do not depend on the
 torch RNG of the machine that reads them. Usage:
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out <directory>   (then copy the files into tests/golden/)
 """
 from __future__ import annotations
 
@@ -94,7 +94,7 @@ def to_np(t: torch.Tensor) -> np.ndarray:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default="gpurun_out/golden")
+    ap.add_argument("--out", required=True, help="directory for the new fixtures")
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
