@@ -344,8 +344,9 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(const ResolveParams a) 
 // Sample and resolve in one pass when no neighbour is read (no spatial reuse, Reset or Static):
 // one thread per image pixel evaluates its ss x ss subpixels' winners (warp-deduplicated),
 // box-filters them and merges the history with resolve.cu:191-258's arithmetic. The samples are
-// still written for inspection.
-__global__ void __launch_bounds__(kBlock) sample_resolve_fused_kernel(const ResolveParams a) {
+// still written for inspection. The pass waits on its dependent gathers (key, then the winner's SH),
+// so it is held to 40 registers for 6 resident blocks per SM.
+__global__ void __launch_bounds__(kBlock, 6) sample_resolve_fused_kernel(const ResolveParams a) {
     advance_frame(a);
     const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
     const bool active = idx < a.n_pixels;
