@@ -48,6 +48,9 @@ DEFAULT_WORKLOAD = "batch_6m_1080_st"
 # DRAM bytes (read + write) of one st_scatter_kernel launch on the default workload, from
 # `ncu --set full` (profiles/st_scatter_kernel_batch_6m_1080.md)
 NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 279.15e6 + 15.66e6}
+# warp instructions of one st_scatter_kernel launch on the default workload, from the same capture:
+# the kernel is bound by instruction issue, so its issue rate is the roofline that explains its time
+NCU_SCATTER_WARP_INSTRUCTIONS = {"batch_6m_1080_st": 467.5e6}
 
 # measured copy bandwidth and bf16 GEMM rate of this pool's B200s when MEASURED_PEAKS.json is absent
 FALLBACK_HBM_GBS = 6650.0
@@ -207,6 +210,20 @@ def algorithmic_bytes(n: int, n_fb: int, n_px: int, unique_winners: int) -> dict
     accumulate = 44 * n + 8 * n_fb
     frame = 44 * n + 48 * n_fb + 48 * n_px + 204 * unique_winners
     return {"accumulate": accumulate, "frame": frame}
+
+
+def issue_roofline(workload: str, acc_ms: float, sms: int, max_mhz: float | None) -> dict | None:
+    """Warp instructions issued per second by the accumulate stage against the SMs' issue limit (4 warp
+    instructions per clock per SM at the maximum SM clock). The count is the scatter kernel's from ncu
+    (the queue kernel's few instructions are left out), the time the stage's live CUDA-event time."""
+    instructions = NCU_SCATTER_WARP_INSTRUCTIONS.get(workload)
+    if instructions is None or not max_mhz:
+        return None
+    peak = sms * 4 * max_mhz * 1e6
+    achieved = instructions / (acc_ms * 1e-3)
+    return {"bound": "issue", "warp_instructions_per_launch": instructions, "achieved": round(achieved / 1e9, 1),
+            "peak": round(peak / 1e9, 1), "unit": "G warp instructions/s", "frac": round(achieved / peak, 4),
+            "source": "ncu smsp__inst_executed.sum of st_scatter_kernel (profiles)"}
 
 
 def run_ours(args, world, rank, local) -> dict | None:
@@ -374,6 +391,8 @@ def run_ours(args, world, rank, local) -> dict | None:
             "traffic": traffic,
             "algorithmic_bytes_per_launch": alg["accumulate"],
             "accumulate_ms": round(acc_ms, 5),
+            "issue": issue_roofline(args.workload, acc_ms, torch.cuda.get_device_properties(dev).multi_processor_count,
+                                    clock_info.get("sm_max_mhz")),
             "frame": {"algorithmic_bytes": alg["frame"], "achieved_gbs": round(alg["frame"] / (ms_per_step * 1e-3) / 1e9, 1),
                       "frac": round(alg["frame"] / (ms_per_step * 1e-3) / 1e9 / peak, 4),
                       "unique_winners": unique},

@@ -47,3 +47,11 @@ def test_peaks_fall_back_without_the_measured_file(bench, tmp_path, monkeypatch)
     (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 6541.5, "bf16_tflops": 1657.2}')
     assert bench.hbm_peak() == (6541.5, "measured")
     assert bench.bf16_peak() == (1657.2, "measured")
+
+
+def test_issue_roofline(bench):
+    r = bench.issue_roofline("batch_6m_1080_st", 0.512, 148, 1965.0)
+    assert r["bound"] == "issue" and r["peak"] == pytest.approx(148 * 4 * 1.965, rel=1e-3)
+    assert r["frac"] == pytest.approx(467.5e6 / 0.512e-3 / (148 * 4 * 1965e6), rel=1e-3)
+    assert bench.issue_roofline("batch_6m_1080_st", 0.512, 148, None) is None
+    assert bench.issue_roofline("st_100k_640_st", 0.1, 148, 1965.0) is None
