@@ -45,12 +45,34 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "batch_6m_1080_st"
 
-# DRAM bytes (read + write) of one st_scatter_kernel launch on the default workload, from
-# `ncu --set full` (profiles/st_scatter_kernel_batch_6m_1080.md)
-NCU_TRAFFIC_BYTES = {"batch_6m_1080_st": 279.15e6 + 15.66e6}
-# warp instructions of one st_scatter_kernel launch on the default workload, from the same capture:
-# the kernel is bound by instruction issue, so its issue rate is the roofline that explains its time
-NCU_SCATTER_WARP_INSTRUCTIONS = {"batch_6m_1080_st": 467.5e6}
+# One `ncu --set full` capture of st_scatter_kernel on the default workload: DRAM bytes (read + write)
+# and warp instructions of one launch, with the digest of the kernel sources the capture ran. When
+# those sources change, the figures no longer describe the kernel: bench then reports them as null
+# ("stale") until a new capture replaces them.
+SCATTER_SOURCES = ("accumulate_st.cu", "sgs_rows.cuh", "sgs_project.cuh", "sgs_common.cuh", "sgs_internal.h")
+NCU_CAPTURE = {
+    "batch_6m_1080_st": {"sources_digest": "72720a37373557db", "dram_bytes": 279.15e6 + 15.66e6,
+                         "warp_instructions": 467.5e6},
+}
+CSRC = ROOT / "stochastic-gaussian-splatting_b200" / "csrc"
+
+
+def scatter_sources_digest() -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in SCATTER_SOURCES:
+        h.update((CSRC / name).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def ncu_capture(workload: str) -> dict | None:
+    """The capture's figures for `workload` if they were measured on the current kernel sources."""
+    cap = NCU_CAPTURE.get(workload)
+    if cap is None or cap["sources_digest"] != scatter_sources_digest():
+        return None
+    return cap
+
 
 # measured copy bandwidth and bf16 GEMM rate of this pool's B200s when MEASURED_PEAKS.json is absent
 FALLBACK_HBM_GBS = 6650.0
@@ -140,12 +162,17 @@ class RawEvents:
         self.rt.cudaEventCreate.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
         self.rt.cudaEventElapsedTime.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.c_void_p]
         self.rt.cudaEventDestroy.argtypes = [ctypes.c_void_p]
+        self.rt.cudaEventRecord.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
 
     def create(self):
         ev = self.ct.c_void_p()
         if self.rt.cudaEventCreate(self.ct.byref(ev)) != 0:
             raise RuntimeError("cudaEventCreate failed")
         return ev
+
+    def record(self, ev, stream_handle: int):
+        if self.rt.cudaEventRecord(ev, self.ct.c_void_p(stream_handle)) != 0:
+            raise RuntimeError("cudaEventRecord failed")
 
     def elapsed_ms(self, start, end) -> float:
         ms = self.ct.c_float()
@@ -216,14 +243,28 @@ def issue_roofline(workload: str, acc_ms: float, sms: int, max_mhz: float | None
     """Warp instructions issued per second by the accumulate stage against the SMs' issue limit (4 warp
     instructions per clock per SM at the maximum SM clock). The count is the scatter kernel's from ncu
     (the queue kernel's few instructions are left out), the time the stage's live CUDA-event time."""
-    instructions = NCU_SCATTER_WARP_INSTRUCTIONS.get(workload)
-    if instructions is None or not max_mhz:
+    cap = ncu_capture(workload)
+    if cap is None or not max_mhz:
         return None
+    instructions = cap["warp_instructions"]
     peak = sms * 4 * max_mhz * 1e6
     achieved = instructions / (acc_ms * 1e-3)
     return {"bound": "issue", "warp_instructions_per_launch": instructions, "achieved": round(achieved / 1e9, 1),
             "peak": round(peak / 1e9, 1), "unit": "G warp instructions/s", "frac": round(achieved / peak, 4),
-            "source": "ncu smsp__inst_executed.sum of st_scatter_kernel (profiles)"}
+            "source": "ncu smsp__inst_executed.sum of st_scatter_kernel on the current sources"}
+
+
+def workload_config(workload: str, n: int, width: int, height: int, fl: dict, world: int, scene_bytes: int) -> dict:
+    """The `config` object of both arms' lines: the same keys and values for the same workload."""
+    return {
+        "workload": f"{workload}: {n} Gaussians, {width}x{height}, supersampling {fl['ss']}, "
+                    f"{'GPS' if fl['gps'] else 'stochastic transparency'}, "
+                    f"{'hybrid' if fl['hybrid'] else 'scatter'} scheduling, 1 spp per step, Static resolve",
+        "gaussians": n, "width": width, "height": height, "supersampling": fl["ss"], "use_gps": fl["gps"],
+        "hybrid_scheduling": fl["hybrid"], "spatial_reuse": False, "parallelism": f"replicas x{world}",
+        "l2": (f"inputs ({scene_bytes / 1e9:.2f} GB) larger than L2 (126 MB), no flush" if scene_bytes > 126e6
+               else f"inputs ({scene_bytes / 1e6:.1f} MB) fit in L2 (126 MB), not flushed"),
+    }
 
 
 def run_ours(args, world, rank, local) -> dict | None:
@@ -355,7 +396,8 @@ def run_ours(args, world, rank, local) -> dict | None:
     peak, peak_kind = hbm_peak()
     scene_bytes = scene_cpu.nbytes()
     achieved = alg["accumulate"] / (acc_ms * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC_BYTES.get(args.workload)
+    capture = ncu_capture(args.workload)
+    traffic = capture["dram_bytes"] if capture else None
     ms_per_step = elapsed_ms / args.steps
     value = replica_throughput(args.steps, world, elapsed_ms)
     line = {
@@ -371,15 +413,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": f"synthetic (seeded {n}-Gaussian scene drawn as the {args.workload} workload; no dataset)",
-        "config": {
-            "workload": f"{args.workload}: {n} Gaussians, {W}x{H}, supersampling {ss}, "
-                        f"{'GPS' if fl['gps'] else 'stochastic transparency'}, "
-                        f"{'hybrid' if fl['hybrid'] else 'scatter'} scheduling, 1 spp per step, Static resolve",
-            "gaussians": n, "width": W, "height": H, "supersampling": ss, "use_gps": fl["gps"],
-            "hybrid_scheduling": fl["hybrid"], "spatial_reuse": False, "parallelism": f"replicas x{world}",
-            "l2": (f"inputs ({scene_bytes / 1e9:.2f} GB) larger than L2 (126 MB), no flush" if scene_bytes > 126e6
-                   else f"inputs ({scene_bytes / 1e6:.1f} MB) fit in L2 (126 MB), not flushed"),
-        },
+        "config": workload_config(args.workload, n, W, H, fl, world, scene_bytes),
         "roofline": {
             "bound": "hbm",
             "kernel": "accumulate stage (st_scatter_kernel + st_queue_kernel)" if not fl["gps"] else "accumulate stage (gps kernels)",
@@ -389,6 +423,9 @@ def run_ours(args, world, rank, local) -> dict | None:
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of st_scatter_kernel, one launch, "
+                               "captured on the current sources") if capture else
+                              "no capture of the current kernel sources (stale figures are not reported)",
             "algorithmic_bytes_per_launch": alg["accumulate"],
             "accumulate_ms": round(acc_ms, 5),
             "issue": issue_roofline(args.workload, acc_ms, torch.cuda.get_device_properties(dev).multi_processor_count,
@@ -408,7 +445,16 @@ def run_ours(args, world, rank, local) -> dict | None:
     if not args.no_batch and args.workload.startswith("batch_6m"):
         line["camera_path"] = camera_path_fps(scene, fl, dev, spp=8)
     if not args.no_batch and args.workload.startswith("batch_6m"):
-        line["batch32_graph"] = batch_graph(scene, fl, dev, steps=max(4, args.steps // 8))
+        line["batch32_graph"] = {
+            "stochastic_transparency": batch_graph(scene, dict(fl, gps=False), dev, steps=max(4, args.steps // 8)),
+            "gps": batch_graph(scene, dict(fl, gps=True), dev, steps=max(4, args.steps // 8)),
+        }
+    if not args.no_reference_cuda and args.workload.startswith("batch_6m"):
+        # the reference's own CUDA backend on this scene and camera, in this process (a baseline leg)
+        line["reference_cuda"] = {
+            "stochastic_transparency": reference_cuda_baseline(scene, cam, dict(fl, gps=False), dev),
+            "gps": reference_cuda_baseline(scene, cam, dict(fl, gps=True), dev),
+        }
     if not (args.no_train and args.no_learned) and args.workload.startswith("batch_6m"):
         del scene
         torch.cuda.empty_cache()
@@ -417,6 +463,9 @@ def run_ours(args, world, rank, local) -> dict | None:
         torch.cuda.empty_cache()
     if not args.no_train and args.workload.startswith("batch_6m"):
         line["train_step"] = train_measure(dev)
+    if not args.no_progressive and args.workload.startswith("batch_6m"):
+        line["progressive_gps_hybrid"] = progressive_measure(dev, reference=not args.no_reference_cuda)
+        torch.cuda.empty_cache()
     probe = atomic_probe(dev)
     line["atomics"] = {"probe": probe}
     if not args.no_cpu_baseline:
@@ -478,12 +527,16 @@ def learned_resolve_measure(dev) -> dict:
     }
 
 
-def train_measure(dev, views: int = 4, target_spp: int = 64, steps_per_view: int = 2) -> dict:
-    """Differentiable training step of the 500k-Gaussian 800x800 workload: 8 samples forward, L1 +
-    0.2 (1 - SSIM), hand-written backward to all parameters, Adam update (targets at 64 spp here)."""
+def train_measure(dev, views: int = 24, target_spp: int = 1024, steps_per_view: int = 2) -> dict:
+    """Differentiable training step of the 500k-Gaussian 800x800 workload: 24 orbit views whose targets
+    are 1024-sample renders of a perturbed copy of the scene; per step 8 samples forward, L1 + 0.2
+    (1 - SSIM), hand-written backward to all parameters, Adam update."""
     import sgs_train
 
+    t_targets = time.perf_counter()
     scene, cams, targets = sgs_train.make_problem(views=views, target_spp=target_spp, device=dev)
+    torch.cuda.synchronize(dev)
+    t_targets = time.perf_counter() - t_targets
     params = [t.to(dev).requires_grad_(True) for t in scene.tensors()]
     opt = torch.optim.Adam(params, lr=1e-3)
     settings = [sgs_train.view_settings(c, dev) for c in cams]
@@ -506,6 +559,7 @@ def train_measure(dev, views: int = 4, target_spp: int = 64, steps_per_view: int
     torch.cuda.synchronize(dev)
     ms = t0.elapsed_time(t1) / n
     return {"gaussians": int(scene.means.shape[0]), "resolution": "800x800", "spp_per_step": 8,
+            "views": views, "target_spp": target_spp, "target_render_s": round(t_targets, 2),
             "ms_per_step": round(ms, 3), "steps_per_s": round(1000.0 / ms, 2),
             "loss_first_epoch": round(sum(losses) / len(losses), 5),
             "loss_last_epoch": round(float(sum(last[-views:]) / views), 5)}
@@ -594,6 +648,170 @@ def batch_graph(scene, fl, dev, steps: int) -> dict:
             "megapixels_per_s_graph": round(pixels / (graph_ms * 1e-3) / 1e6, 1)}
 
 
+def reference_cuda_baseline(scene, cam, fl, dev, calls: int = 32, rounds: int = 2) -> dict:
+    """The reference's own CUDA backend, its unmodified `_C.render` built from its sources into
+    oracle/_ref/C, on the same scene, camera, flags and Static loop as this library's `_C.render`, in
+    this process on this GPU. A baseline leg like `cpu_baseline`: the measured path never touches it.
+    CUDA events around `calls` calls after 4 warm-up calls; the two implementations alternate for
+    `rounds` rounds and each keeps its fastest round."""
+    from oracle import build_ref
+
+    if not build_ref.available():
+        return {"unavailable": "the reference extension was not built under oracle/_ref (oracle/build_ref.py)"}
+    from StochasticGSCudaBackend import _C
+
+    ref_C, _ = build_ref.load()
+    W, H, ss = cam.width, cam.height, fl["ss"]
+    n_fb = W * H * ss * ss
+    kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device=dev), torch.empty((0, n_fb, 4), device=dev))
+    e = torch.empty(0)
+    w2c, pos, eye = cam.w2c.to(dev), cam.position.to(dev), torch.eye(4, device=dev)
+    blue = torch.empty(0, dtype=torch.uint8, device=dev)
+
+    def args(hist, mode):
+        return (*scene.tensors(), w2c, pos, W, H, cam.focal_x, cam.focal_y, cam.center_x, cam.center_y,
+                cam.near_plane, cam.far_plane, fl["aa"], ss, fl["gps"], fl["hybrid"], False, blue, *kb, *hist, eye,
+                mode)
+
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(render) -> float:
+        hist = render(*args((e, e, e, e), 0))
+        for _ in range(4):
+            hist = render(*args(hist, 1))
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        t0.record(stream)
+        for _ in range(calls):
+            hist = render(*args(hist, 1))
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        return t0.elapsed_time(t1) / calls
+
+    ref_ms, our_ms = [], []
+    for _ in range(rounds):
+        ref_ms.append(timed(ref_C.render))
+        our_ms.append(timed(_C.render))
+    r, o = min(ref_ms), min(our_ms)
+    return {"implementation": "reference _C.render built from its sources (oracle/_ref/C), same process and GPU",
+            "workload": f"{scene.means.shape[0]} Gaussians, {W}x{H}, ss {ss}, {'GPS' if fl['gps'] else 'ST'}, "
+                        f"{'hybrid' if fl['hybrid'] else 'scatter'}, Static",
+            "calls": calls, "rounds": rounds, "reference_ms_per_sample": round(r, 5), "ours_ms_per_sample": round(o, 5),
+            "reference_sample_frames_per_s": round(1000.0 / r, 2), "ours_sample_frames_per_s": round(1000.0 / o, 2),
+            "ratio": round(r / o, 3), "same_box": True}
+
+
+def progressive_measure(dev, views: int = 16, spp: int = 16, reference: bool = True) -> dict:
+    """The GPS-hybrid progressive workload: 1M Gaussians with heavy-tailed footprints (log-scales
+    N(-3, 1^2)), 1280x720 with supersampling 2, GPS with hybrid scheduling capped at 1024 points per
+    Gaussian and 65,536 queued Gaussians, 16 orbit views at radius 4, 16 samples per view: the first
+    sample of a view in Reproject (Reset for the first view), the others Static, spatial reuse on
+    (Renderer.py:74-97). One untimed pass over the first view, then all 256 samples timed with CUDA
+    events per call; the sample/resolve passes of each Reproject sample timed from the event the
+    library records after its accumulate stage. The reference arm runs the same loop on the
+    reference extension built with those two caps (oracle/build_ref.py)."""
+    from StochasticGSCudaBackend import _C
+
+    W, H, ss = 1280, 720, 2
+    max_fragments, max_binned = 1024, 65536
+    scene = sgs_scenes.make_scene(sgs_scenes.SCENES["gps_1m"], seed=0).to(dev)
+    cams = sgs_scenes.orbit_cameras(views, 4.0, W, H)
+    n_fb, n_px = W * H * ss * ss, W * H
+    e = torch.empty(0)
+    blue = torch.empty(0, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    cam_t = [(c.w2c.to(dev), c.position.to(dev)) for c in cams]
+    v2pv = [torch.eye(4, device=dev)] + [
+        (cams[i - 1].w2c.double() @ torch.linalg.inv(cams[i].w2c.double())).float().to(dev) for i in range(1, views)]
+
+    def args(v, kb, hist, mode):
+        c = cams[v]
+        return (*scene.tensors(), *cam_t[v], W, H, c.focal_x, c.focal_y, c.center_x, c.center_y, c.near_plane,
+                c.far_plane, False, ss, True, True, True, blue, *kb, *hist, v2pv[v], mode)
+
+    raw = RawEvents()
+
+    def run(render, kwargs, timed: bool, n_views: int, stage_events: bool):
+        kb = (torch.full((4, n_fb, 2), -1, dtype=torch.int32, device=dev), torch.zeros((4, n_fb, 4), device=dev))
+        hist = (e, e, e, e)
+        marks = []
+        for v in range(n_views):
+            for s in range(spp):
+                mode = (0 if v == 0 else 2) if s == 0 else 1
+                if timed:
+                    ev = [raw.create() for _ in range(4)]  # call start, accumulate start/end, call end
+                    if stage_events:
+                        _C.set_stage_events(ev[1], ev[2])
+                    raw.record(ev[0], stream.cuda_stream)
+                hist = render(*args(v, kb, hist, mode), **kwargs)
+                if timed:
+                    raw.record(ev[3], stream.cuda_stream)
+                    marks.append((mode, ev))
+        _C.set_stage_events(None, None)
+        torch.cuda.synchronize(dev)
+        if not timed:
+            return None
+        mean = lambda xs: sum(xs) / len(xs)
+        rep = [ev for mode, ev in marks if mode == 2]
+        out = {"ms_per_sample": mean([raw.elapsed_ms(ev[0], ev[3]) for _, ev in marks]),
+               "reproject_ms_per_sample": mean([raw.elapsed_ms(ev[0], ev[3]) for ev in rep])}
+        if stage_events:
+            out["accumulate_ms"] = mean([raw.elapsed_ms(ev[1], ev[2]) for _, ev in marks])
+            out["reproject_resolve_ms"] = mean([raw.elapsed_ms(ev[2], ev[3]) for ev in rep])
+            out["static_resolve_ms"] = mean([raw.elapsed_ms(ev[2], ev[3]) for mode, ev in marks if mode == 1])
+        for _, ev in marks:
+            for x in ev:
+                raw.destroy(x)
+        return out
+
+    kwargs = dict(max_fragments=max_fragments, max_binned=max_binned)
+    run(_C.render, kwargs, timed=False, n_views=1, stage_events=False)
+    ours = run(_C.render, kwargs, timed=True, n_views=views, stage_events=True)
+    # distinct winners of one sample of the second view, for the algorithmic bytes of the sample and
+    # resolve passes: per framebuffer subpixel the winner key 8, samples written and read 32, reuse
+    # weights written and read 32, the k-buffer (4 entries of 24 B) read and rewritten 192; per pixel
+    # the Reproject history read 20 and the outputs written 24; per distinct winner its geometry
+    # re-projected 44 and its mean and SH 204 (the means counted once: 236)
+    kb = (torch.full((4, n_fb, 2), -1, dtype=torch.int32, device=dev), torch.zeros((4, n_fb, 4), device=dev))
+    _, ws, layout = _C.render_with_workspace(*args(1, kb, (e, e, e, e), 0), **kwargs)
+    fb = _C.workspace_views(ws, layout, n_fb, True)["framebuffer"]
+    unique = int(torch.unique(fb[fb != -1] & 0xFFFFFFFF).numel())
+    del ws, fb, kb
+    resolve_bytes = 264 * n_fb + 44 * n_px + 236 * unique
+    peak, peak_kind = hbm_peak()
+    gbs = resolve_bytes / (ours["reproject_resolve_ms"] * 1e-3) / 1e9
+    result = {
+        "workload": f"1M heavy-tailed Gaussians, {W}x{H} ss {ss}, GPS hybrid (max_fragments {max_fragments}, "
+                    f"max_binned {max_binned}), spatial reuse, {views} orbit views x {spp} samples, Reproject "
+                    f"between views, Static within a view",
+        "ms_per_sample": round(ours["ms_per_sample"], 4),
+        "sample_frames_per_s": round(1000.0 / ours["ms_per_sample"], 2),
+        "reproject_ms_per_sample": round(ours["reproject_ms_per_sample"], 4),
+        "accumulate_ms": round(ours["accumulate_ms"], 4),
+        "static_resolve_ms": round(ours["static_resolve_ms"], 4),
+        "reproject_resolve": {"ms": round(ours["reproject_resolve_ms"], 4), "algorithmic_bytes": resolve_bytes,
+                              "unique_winners": unique, "achieved_gbs": round(gbs, 1), "peak": peak,
+                              "peak_source": f"{peak_kind} hbm_gbs", "frac": round(gbs / peak, 4)},
+    }
+    if reference:
+        from oracle import build_ref
+
+        if build_ref.available():
+            ref_c1 = build_ref.load_c1()
+            run(ref_c1.render, {}, timed=False, n_views=1, stage_events=False)
+            theirs = run(ref_c1.render, {}, timed=True, n_views=views, stage_events=False)
+            result["reference_cuda"] = {
+                "implementation": "reference _C.render built from its sources with the workload's two caps "
+                                  "(oracle/_ref/c1), same process and GPU",
+                "ms_per_sample": round(theirs["ms_per_sample"], 4),
+                "reproject_ms_per_sample": round(theirs["reproject_ms_per_sample"], 4),
+                "ratio": round(theirs["ms_per_sample"] / ours["ms_per_sample"], 3), "same_box": True}
+        else:
+            result["reference_cuda"] = {"unavailable": "the reference extension was not built under oracle/_ref"}
+    del scene
+    return result
+
+
 def cpu_baseline(scene_cpu, cam, fl, frames: int, workload: str) -> tuple[dict, dict]:
     """The C++ restatement of the reference path (oracle/) on all host cores, a bounded sample."""
     from oracle import cpu
@@ -678,8 +896,8 @@ def run_reference(args, world, rank) -> dict | None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded 6M-Gaussian scene)",
-        "config": {"workload": args.workload, "gaussians": int(scene_cpu.means.shape[0]), "width": cam.width,
-                   "height": cam.height, "parallelism": "host cores"},
+        "config": workload_config(args.workload, int(scene_cpu.means.shape[0]), cam.width, cam.height, fl, world,
+                                  scene_cpu.nbytes()),
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full sample-frames of {args.workload}: the C++ restatement of the "
                                    f"reference kernels (the reference has no CPU path)"},
@@ -699,6 +917,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 32-view CUDA-graph measurement")
     ap.add_argument("--no-train", action="store_true", help="skip the differentiable training-step measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-resolve measurement")
+    ap.add_argument("--no-progressive", action="store_true",
+                    help="skip the GPS-hybrid progressive workload (16 views x 16 samples, reuse, Reproject)")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the timing of the reference's own CUDA backend in this process")
     args = ap.parse_args()
     if args.impl == "reference":
         # reference semantics on the host cores; no GPU work, no process group needed

@@ -162,12 +162,16 @@ int sgs_render_samples(const sgs_gaussians* gaussians, const sgs_camera* camera,
  * counterpart in the reference. The caller passes inputs, history and outputs as for sgs_render;
  * the scratch lives in a fixed 64 MiB device array of the library instead of a caller workspace,
  * so nothing is allocated per call. That array is held by every CUDA context that loads it, until
- * the process exits. The first call on each device (that device current) looks up the array's
- * device address; make it before any stream capture. All calls on a device share the array: the
- * render clears what must start empty, but calls that can overlap on the GPU race and must be
- * ordered by the caller. Renders needing more than 64 MiB of scratch (sgs_workspace_size) are
- * rejected with SGS_ERROR_WORKSPACE before any launch; 1920x1080 without supersampling or spatial
- * reuse fits. */
+ * the process exits. Every call looks up the array's device address in the context current on the
+ * calling thread, so the address is valid for that context (also after cudaDeviceReset, or under a
+ * caller's own driver context); the first call in a context may load the module: make it before
+ * any stream capture. All calls on a device share the array: the render clears what must start
+ * empty, but calls that can overlap on the GPU race and must be ordered by the caller. Renders
+ * needing more than 64 MiB of scratch (sgs_workspace_size) are rejected with SGS_ERROR_WORKSPACE
+ * before any launch. Stochastic transparency at 1920x1080 without supersampling or spatial reuse
+ * fits for any scene size; hybrid GPS at 1920x1080 fits up to about 289,000 queue entries
+ * (max_binned, by default min(N, 2^20)), so larger scenes need settings->max_binned at or below
+ * that. */
 int sgs_render_no_alloc(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
                         const sgs_history* history, const sgs_outputs* outputs, void* stream);
 

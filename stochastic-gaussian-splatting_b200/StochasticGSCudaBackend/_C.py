@@ -134,7 +134,8 @@ def _ptr(t: torch.Tensor | None) -> int | None:
 def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, width, height, focal_x, focal_y,
              center_x, center_y, near_plane, far_plane, proper_antialiasing, supersampling_factor_raw, use_gps,
              hybrid_scheduling, spatial_reuse, blue_noise, k_buffer_primitives, k_buffer_occlusion, history_image,
-             history_depth, history_alpha, history_weight_mass, view_to_previous_view, temporal_mode, preactivated=None):
+             history_depth, history_alpha, history_weight_mass, view_to_previous_view, temporal_mode, preactivated=None,
+             max_fragments=0, max_binned=0):
     _check(isinstance(means, torch.Tensor) and means.is_cuda, "means must be a CUDA tensor")
     device = means.device
     means = _cuda_f32(means, "means", device)
@@ -196,13 +197,16 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
                and preactivated.dtype == torch.float32 and tuple(preactivated.shape) == (n, 8)
                and preactivated.is_contiguous() and preactivated.data_ptr() % 16 == 0,
                "preactivated must be the contiguous (N, 8) float32 CUDA tensor of preactivate()")
+    max_fragments, max_binned = int(max_fragments or 0), int(max_binned or 0)
+    _check(0 <= max_fragments < 2 ** 32 and 0 <= max_binned < 2 ** 32,
+           "max_fragments and max_binned must be non-negative 32-bit counts (0 = the reference's default)")
     g = _abi.Gaussians(_ptr(means), _ptr(scales), _ptr(rotations), _ptr(opacities), _ptr(sh_coefficients), n, sh_bases,
                        _ptr(preactivated))
     c = _abi.Camera(w2c.data_ptr(), cam_position.data_ptr(), width, height, float(focal_x), float(focal_y),
                     float(center_x), float(center_y), float(near_plane), float(far_plane))
     s = _abi.SettingsC(int(bool(proper_antialiasing)), ss, int(bool(use_gps)), int(bool(hybrid_scheduling)),
-                       int(bool(spatial_reuse)), mode, _ptr(blue_noise), _ptr(view_to_previous_view), 0, 0,
-                       _device_frame_pointer(device))
+                       int(bool(spatial_reuse)), mode, _ptr(blue_noise), _ptr(view_to_previous_view), max_fragments,
+                       max_binned, _device_frame_pointer(device))
     h = _abi.HistoryC(
         _ptr(history_image) if mode else None, _ptr(history_depth) if mode else None,
         _ptr(history_alpha) if mode else None, _ptr(history_weight_mass) if mode else None,
@@ -213,8 +217,8 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
     return device, g, c, s, h, (width, height), keep
 
 
-def _render_impl(args, want_workspace: bool, streams=None, preactivated=None):
-    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated)
+def _render_impl(args, want_workspace: bool, streams=None, preactivated=None, caps=None):
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated, **(caps or {}))
     with torch.cuda.device(device):
         opts = dict(dtype=torch.float32, device=device)
         image = torch.empty((height, width, 3), **opts)
@@ -256,16 +260,25 @@ def _render_impl(args, want_workspace: bool, streams=None, preactivated=None):
         return (image, depth, alpha, weight_mass), workspace, layout
 
 
-def render(*args, preactivated=None):
+def render(*args, preactivated=None, max_fragments=0, max_binned=0):
     """`_C.render` with the reference's 29 positional arguments; returns (image, depth, alpha, weight_mass).
-    `preactivated` (keyword only, not in the reference): the (N, 8) tensor of `preactivate()` for
-    these Gaussians; the accumulate pass then reads covariance and opacity from it (same bits)."""
+
+    Keyword-only extras (not in the reference's binding):
+      preactivated   the (N, 8) tensor of `preactivate()` for these Gaussians; the accumulate pass then
+                     reads covariance and opacity from it (same bits);
+      max_fragments  GPS points per Gaussian cap of hybrid scheduling (0: the reference's
+                     round(W_fb * H_fb / (2 ss^2)), accumulate_hybrid_gps.cu:86);
+      max_binned     capacity of the hybrid work queue in Gaussians (0: the reference's min(N, 2^20),
+                     accumulate_hybrid_gps.cu:22 and accumulate_hybrid.cu:27). Gaussians beyond it are
+                     rendered in place, as in the reference."""
     if len(args) != 29:
         raise TypeError(f"render() takes 29 positional arguments ({len(args)} given)")
-    return _render_impl(args, want_workspace=False, preactivated=preactivated)
+    return _render_impl(args, want_workspace=False, preactivated=preactivated,
+                        caps=dict(max_fragments=max_fragments, max_binned=max_binned))
 
 
-def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cuda.Stream, *args, preactivated=None):
+def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cuda.Stream, *args, preactivated=None,
+                 max_fragments=0, max_binned=0):
     """As `render` (the same 29 arguments after the two streams), with the clear and accumulate passes
     enqueued on `accumulate_stream` and the sample and resolve passes on `resolve_stream` (the C ABI's
     sgs_render_split): a following call can accumulate while this one resolves. The outputs are
@@ -273,7 +286,7 @@ def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cud
     if len(args) != 29:
         raise TypeError(f"render_split() takes 2 streams and 29 positional arguments ({len(args)} given)")
     return _render_impl(args, want_workspace=False, streams=(accumulate_stream, resolve_stream),
-                        preactivated=preactivated)
+                        preactivated=preactivated, caps=dict(max_fragments=max_fragments, max_binned=max_binned))
 
 
 def render_samples(n_samples: int, *args, preactivated=None):
@@ -328,16 +341,17 @@ def _render_samples_impl(n: int, args, want_workspace: bool, preactivated=None):
     return outs, workspace, layout
 
 
-def workspace_size(*args) -> int:
+def workspace_size(*args, max_fragments=0, max_binned=0) -> int:
     """Bytes of scratch a render with these 29 `render` arguments needs (sgs_workspace_size)."""
-    _, g, c, s, _, _, _ = _prepare(*args)
+    _, g, c, s, _, _, _ = _prepare(*args, max_fragments=max_fragments, max_binned=max_binned)
     n = int(_lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s)))
     if n == 0:
         raise RuntimeError(_abi.last_error(_lib) or "invalid render arguments")
     return n
 
 
-def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=None) -> None:
+def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=None, max_fragments=0,
+                max_binned=0) -> None:
     """Renders like `render` into caller-owned buffers: `outputs` = (image (H, W, 3), depth, alpha,
     weight_mass (H, W, 1)) float32 CUDA tensors, `workspace` a uint8 CUDA tensor of at least
     `workspace_size(*args)` bytes (256-byte aligned), `streams` = None (current stream) or
@@ -345,7 +359,8 @@ def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=N
     be captured in a CUDA graph with fixed buffers (for example ping-ponged histories)."""
     if len(args) != 29:
         raise TypeError(f"render_into() takes outputs, workspace, streams and 29 render arguments ({len(args)} given)")
-    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated)
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated, max_fragments=max_fragments,
+                                                         max_binned=max_binned)
     shapes = ((height, width, 3), (height, width, 1), (height, width, 1), (height, width, 1))
     for name, t, shape in zip(("image", "depth", "alpha", "weight_mass"), outputs, shapes):
         _check(isinstance(t, torch.Tensor) and t.is_cuda and t.device == device and t.dtype == torch.float32
@@ -369,11 +384,12 @@ def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=N
     del keep
 
 
-def render_with_workspace(*args, preactivated=None):
+def render_with_workspace(*args, preactivated=None, max_fragments=0, max_binned=0):
     """As `render`, plus the workspace tensor and its layout (winner framebuffer, samples, reuse weights)."""
     if len(args) != 29:
         raise TypeError(f"render_with_workspace() takes 29 positional arguments ({len(args)} given)")
-    return _render_impl(args, want_workspace=True, preactivated=preactivated)
+    return _render_impl(args, want_workspace=True, preactivated=preactivated,
+                        caps=dict(max_fragments=max_fragments, max_binned=max_binned))
 
 
 def workspace_views(workspace: torch.Tensor, layout, n_fb: int, spatial_reuse: bool) -> dict[str, torch.Tensor]:

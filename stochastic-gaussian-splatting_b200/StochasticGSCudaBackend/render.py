@@ -15,21 +15,21 @@ from StochasticGSCudaBackend import _C  # noqa
 
 
 class Settings(NamedTuple):
-    w2c: torch.Tensor  # affine transformation from model/world space to view space
-    cam_position: torch.Tensor  # camera position in world space
-    width: int  # width of the image plane in pixels
-    height: int  # height of the image plane in pixels
-    focal_x: float  # focal length in x direction in pixels
-    focal_y: float  # focal length in y direction in pixels
-    center_x: float  # x coordinate of the image center in pixels (positive -> right)
-    center_y: float  # y coordinate of the image center in pixels (positive -> down)
-    near_plane: float  # near clipping plane distance
-    far_plane: float  # far clipping plane distance
-    proper_antialiasing: bool  # whether to use proper antialiasing
-    supersampling_factor: int  # factor for supersampling (2 -> render 2x2 subpixels)
-    use_gps: bool  # whether to use Gaussian point splatting
-    hybrid_scheduling: bool  # whether to process large Gaussians in a separate load-balanced pass
-    spatial_reuse: bool  # whether to resample from the four neighbors of each (sub)pixel
+    w2c: torch.Tensor  # world-to-camera matrix, rows of 4 floats (OpenCV axes: x right, y down, z forward)
+    cam_position: torch.Tensor  # (3,) eye point in world coordinates, the origin of the SH view direction
+    width: int  # output image columns
+    height: int  # output image rows
+    focal_x: float  # horizontal focal length, in pixels
+    focal_y: float  # vertical focal length, in pixels
+    center_x: float  # principal point column, in pixels from the left edge
+    center_y: float  # principal point row, in pixels from the top edge
+    near_plane: float  # Gaussians closer than this view depth are culled
+    far_plane: float  # Gaussians beyond this view depth are culled; background depth for reprojection
+    proper_antialiasing: bool  # smaller screen-space dilation with opacity compensation
+    supersampling_factor: int  # s: each output pixel averages s x s framebuffer subpixels
+    use_gps: bool  # splat Poisson-distributed points instead of stochastic transparency
+    hybrid_scheduling: bool  # hand large footprints to a load-balanced work queue
+    spatial_reuse: bool  # also resample each subpixel's four neighbours through the k-buffer
 
     def as_tuple(self) -> tuple:
         return (
@@ -52,16 +52,16 @@ class Settings(NamedTuple):
 
 
 class TemporalMode(IntEnum):
-    RESET = 0  # discard the history
-    STATIC = 1  # same camera as the history: weighted cumulative average
-    REPROJECT = 2  # moving camera: reprojected history with soft rejection
+    RESET = 0  # start over: the history is not read
+    STATIC = 1  # unchanged camera: running average weighted by weight_mass
+    REPROJECT = 2  # camera moved: history warped by view_to_previous_view, rejected where it disagrees
 
 
 class History(NamedTuple):
-    image: torch.Tensor  # (H, W, 3) color premultiplied by alpha
-    depth: torch.Tensor  # (H, W, 1) depth premultiplied by alpha
-    alpha: torch.Tensor  # (H, W, 1)
-    weight_mass: torch.Tensor  # (H, W, 1) accumulated resampling weight
+    image: torch.Tensor  # (H, W, 3) premultiplied RGB (multiplied by alpha)
+    depth: torch.Tensor  # (H, W, 1) premultiplied view depth
+    alpha: torch.Tensor  # (H, W, 1) coverage
+    weight_mass: torch.Tensor  # (H, W, 1) total sample weight merged into this pixel so far
 
 
 BLUE_NOISE_FILE = "stbn_scalar_128x128x64.bin"
@@ -69,7 +69,8 @@ BLUE_NOISE_FILE = "stbn_scalar_128x128x64.bin"
 
 @cache
 def blue_noise() -> torch.Tensor:
-    """Returns the blue noise (64, 128, 128) stored next to the extension, or an empty tensor (white noise)."""
+    """The (64, 128, 128) uint8 spatio-temporal blue-noise volume if its file sits next to `_C`; otherwise an
+    empty tensor, which selects hashed white-noise thresholds."""
     path = Path(_C.__file__).parent / BLUE_NOISE_FILE
     if not path.is_file():
         return torch.empty(0, dtype=torch.uint8, device='cuda')
@@ -77,7 +78,8 @@ def blue_noise() -> torch.Tensor:
 
 
 def create_k_buffer(settings: Settings) -> tuple[torch.Tensor, torch.Tensor]:
-    """Returns empty k-buffers: primitive index and depth, occlusion factors towards the four neighbors."""
+    """Fresh k-buffer state for `settings`: (K, P_fb, 2) int32 entries of (Gaussian index, depth bits), all -1,
+    and (K, P_fb, 4) float32 occlusion ratios towards the four neighbours; K = 0 without spatial reuse."""
     n_entries = (_C.k_buffer_size if settings.spatial_reuse else 0,
                  settings.width * settings.height * settings.supersampling_factor ** 2)
     return (
@@ -99,10 +101,13 @@ def render(
     temporal_mode: TemporalMode,
     *,
     preactivated: torch.Tensor | None = None,
+    max_fragments: int = 0,
+    max_binned: int = 0,
 ) -> History:
-    """One sample-frame (render.py:72-96 of the reference). `preactivated` (keyword only, an
-    addition): the `_C.preactivate(scales, rotations, opacities)` tensor of these Gaussians, read by
-    the accumulate pass in place of the per-sample covariance and sigmoid (same bits)."""
+    """One sample-frame (render.py:72-96 of the reference). Keyword-only additions: `preactivated`, the
+    `_C.preactivate(scales, rotations, opacities)` tensor of these Gaussians, read by the accumulate
+    pass in place of the per-sample covariance and sigmoid (same bits); `max_fragments` and
+    `max_binned`, the GPS point cap and the hybrid queue capacity (0 keeps the reference's values)."""
     return History(*_C.render(
         means,
         scales,
@@ -116,4 +121,6 @@ def render(
         view_to_previous_view,
         int(temporal_mode),
         preactivated=preactivated,
+        max_fragments=max_fragments,
+        max_binned=max_binned,
     ))

@@ -12,17 +12,23 @@
 //  * the array is a file-scope __device__ variable: a CUDA context that loads this file's module
 //    holds it until the process exits (with lazy module loading, from the first call on that
 //    device);
-//  * host code cannot use the array's name as a device address, so the first call on each device
-//    (with that device current) looks the address up with cudaGetSymbolAddress and keeps it; make
-//    that first call outside any stream capture, since the lookup may load the module;
+//  * host code cannot use the array's name as a device address. Every call looks the address up
+//    with cudaGetSymbolAddress in the context current on the calling thread and checks the result,
+//    so the address is always the one of the context the kernels run in: after cudaDeviceReset, or
+//    for a caller that renders under its own driver context, the next call finds the array where
+//    that context placed it (an address kept from an earlier context would dangle). The first call
+//    in a context may load the module there: make it outside any stream capture;
 //  * every call on a device shares the one array and it keeps the previous call's contents; the
 //    render clears the parts that must start empty (framebuffer and queue counters) itself, so
 //    nothing needs clearing by the caller, but calls that can overlap on the GPU (different
 //    streams or threads without ordering) race on the array and must be serialised by the caller;
 //  * requests whose scratch exceeds kScratchBytes are rejected with SGS_ERROR_WORKSPACE before any
-//    launch (1920x1080 without supersampling or spatial reuse fits for any scene size).
+//    launch. Stochastic transparency at 1920x1080 without supersampling or spatial reuse fits for
+//    any scene size: at most 65.5 MB (framebuffer 16.6 MB, samples 33.2 MB, a work queue of at
+//    most 2^18 entries of 60 bytes, 15.7 MB). Hybrid GPS sizes its work queue by max_binned
+//    instead (by default min(N, 2^20) entries of 60 bytes): at 1920x1080 it fits up to about
+//    289,000 entries, so scenes with more Gaussians need settings->max_binned at or below that.
 // No cudaMalloc, cudaFree or allocating library routine is called.
-#include <atomic>
 #include <cuda_runtime.h>
 #include "../../include/sgs_b200.h"
 #include "sgs_internal.h"
@@ -30,11 +36,7 @@
 namespace {
 
 constexpr size_t kScratchBytes = size_t(64) << 20;  // 64 MiB
-constexpr int kMaxDevices = 64;
-
 __device__ __align__(256) unsigned char g_no_alloc_scratch[kScratchBytes];
-
-std::atomic<void*> g_scratch_address[kMaxDevices];
 
 }  // namespace
 
@@ -47,18 +49,10 @@ extern "C" int sgs_render_no_alloc(const sgs_gaussians* gaussians, const sgs_cam
         return sgs::record_error(SGS_ERROR_WORKSPACE,
                                  "sgs_render_no_alloc: this render needs %zu bytes of scratch, the fixed "
                                  "array holds %zu (use sgs_render with a workspace)", need, kScratchBytes);
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
-        return sgs::record_error(SGS_ERROR_CUDA, "sgs_render_no_alloc: no usable current device");
-    void* scratch = g_scratch_address[device].load(std::memory_order_acquire);
-    if (scratch == nullptr) {
-        void* address = nullptr;
-        const cudaError_t err = cudaGetSymbolAddress(&address, g_no_alloc_scratch);
-        if (err != cudaSuccess || address == nullptr)
-            return sgs::record_error(SGS_ERROR_CUDA, "sgs_render_no_alloc: cudaGetSymbolAddress failed: %s",
-                                     cudaGetErrorString(err));
-        g_scratch_address[device].store(address, std::memory_order_release);
-        scratch = address;
-    }
+    void* scratch = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&scratch, g_no_alloc_scratch);
+    if (err != cudaSuccess || scratch == nullptr)
+        return sgs::record_error(SGS_ERROR_CUDA, "sgs_render_no_alloc: cudaGetSymbolAddress failed: %s",
+                                 cudaGetErrorString(err));
     return sgs_render(gaussians, camera, settings, history, outputs, scratch, kScratchBytes, stream);
 }

@@ -50,16 +50,21 @@ def view_settings(cam: sgs_scenes.Camera, device) -> Settings:
 
 
 @torch.no_grad()
-def render_target(tensors, settings: Settings, spp: int, first_frame: int) -> torch.Tensor:
+def render_target(tensors, settings: Settings, spp: int, first_frame: int, samples_per_call: int = 64) -> torch.Tensor:
+    """The plain progressive average of `spp` samples (frames first_frame .. first_frame + spp - 1), rendered
+    `samples_per_call` at a time (the same bits as one `_C.render` call per sample)."""
     e = torch.empty(0)
     hist = (e, e, e, e)
     dev = tensors[0].device
     n_fb = settings.width * settings.height
     kb = (torch.empty((0, n_fb, 2), dtype=torch.int32, device=dev), torch.empty((0, n_fb, 4), device=dev))
-    for s in range(spp):
-        _C.set_frame_index(first_frame + s)
-        hist = _C.render(*tensors, *settings.as_tuple(), torch.empty(0, dtype=torch.uint8, device=dev), *kb, *hist,
-                         torch.eye(4, device=dev), 0 if s == 0 else 1)
+    _C.set_frame_index(first_frame)
+    done = 0
+    while done < spp:
+        n = min(samples_per_call, spp - done)
+        hist = _C.render_samples(n, *tensors, *settings.as_tuple(), torch.empty(0, dtype=torch.uint8, device=dev),
+                                 *kb, *hist, torch.eye(4, device=dev), 0 if done == 0 else 1)
+        done += n
     return hist[0]
 
 

@@ -78,3 +78,17 @@ def mismatch_report(name: str, got: np.ndarray, want: np.ndarray) -> str:
 def assert_bitwise(name: str, got, want):
     msg = mismatch_report(name, got, want)
     assert msg == "", msg
+
+
+# The reference binding seeds every render with a process-global counter (render.cu:56-57) that
+# starts at 0 in each loaded copy of the extension and advances by one per call. Tests that call a
+# reference module's `render` go through this helper so that they all know the frame it used.
+_reference_calls: dict[str, int] = {}
+
+
+def reference_render(module, *args):
+    """Calls `module.render(*args)` (a reference extension); returns (frame index it used, outputs)."""
+    frame = _reference_calls.get(module.__name__, 0)
+    out = module.render(*args)
+    _reference_calls[module.__name__] = frame + 1
+    return frame, out

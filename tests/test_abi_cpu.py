@@ -138,7 +138,8 @@ def test_python_module_mirrors_the_reference_binding():
                           "history", "view_to_previous_view", "temporal_mode"]
     # additions are keyword-only with defaults, so every reference call binds unchanged
     extras = [p for p in params if p.kind is inspect.Parameter.KEYWORD_ONLY]
-    assert [p.name for p in extras] == ["preactivated"] and all(p.default is None for p in extras)
+    assert [p.name for p in extras] == ["preactivated", "max_fragments", "max_binned"]
+    assert [p.default for p in extras] == [None, 0, 0]
     assert callable(create_k_buffer)
     with pytest.raises(TypeError):
         _C.render(1, 2, 3)
@@ -146,3 +147,23 @@ def test_python_module_mirrors_the_reference_binding():
     with pytest.raises(RuntimeError, match="CUDA"):
         _C.render(cpu, cpu, cpu, cpu, cpu, cpu, cpu, 4, 4, 1.0, 1.0, 2.0, 2.0, 0.1, 10.0, False, 1, False, False,
                   False, torch.empty(0), cpu, cpu, cpu, cpu, cpu, cpu, cpu, 0)
+
+
+def test_no_alloc_scratch_bounds_hold():
+    """The fixed 64 MiB scratch of sgs_render_no_alloc holds what its documentation says: stochastic
+    transparency at 1920x1080 for any scene size, hybrid GPS at 1920x1080 up to about 289,000 queue
+    entries (max_binned), and not the hybrid-GPS default queue of a 1M-Gaussian scene."""
+    lib = _abi.load()
+    limit = 64 << 20
+
+    def size(n, gps, hybrid, max_binned=0):
+        g, c, s = _args(n=n, width=1920, height=1080, gps=gps, hybrid=hybrid)
+        s.max_binned = max_binned
+        return lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s))
+
+    for n in (1000, 1 << 18, 6_000_000, 0xFFFFFFFF):
+        assert 0 < size(n, 0, 0) <= limit
+        assert 0 < size(n, 0, 1) <= limit
+    assert size(285_000, 1, 1) <= limit < size(295_000, 1, 1)
+    assert size(6_000_000, 1, 1, max_binned=285_000) <= limit
+    assert size(1_000_000, 1, 1) > limit

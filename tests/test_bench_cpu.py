@@ -49,9 +49,32 @@ def test_peaks_fall_back_without_the_measured_file(bench, tmp_path, monkeypatch)
     assert bench.bf16_peak() == (1657.2, "measured")
 
 
-def test_issue_roofline(bench):
+def test_issue_roofline(bench, monkeypatch):
+    monkeypatch.setitem(bench.NCU_CAPTURE, "batch_6m_1080_st",
+                        {"sources_digest": bench.scatter_sources_digest(), "dram_bytes": 1.0,
+                         "warp_instructions": 467.5e6})
     r = bench.issue_roofline("batch_6m_1080_st", 0.512, 148, 1965.0)
     assert r["bound"] == "issue" and r["peak"] == pytest.approx(148 * 4 * 1.965, rel=1e-3)
     assert r["frac"] == pytest.approx(467.5e6 / 0.512e-3 / (148 * 4 * 1965e6), rel=1e-3)
     assert bench.issue_roofline("batch_6m_1080_st", 0.512, 148, None) is None
     assert bench.issue_roofline("st_100k_640_st", 0.1, 148, 1965.0) is None
+
+
+def test_capture_of_other_kernel_sources_is_not_reported(bench, monkeypatch):
+    """ncu figures measured on other scatter-kernel sources are stale: bench reports none of them."""
+    monkeypatch.setitem(bench.NCU_CAPTURE, "batch_6m_1080_st",
+                        {"sources_digest": "0" * 16, "dram_bytes": 1.0, "warp_instructions": 1.0})
+    assert bench.ncu_capture("batch_6m_1080_st") is None
+    assert bench.issue_roofline("batch_6m_1080_st", 0.512, 148, 1965.0) is None
+
+
+def test_both_arms_describe_the_workload_alike(bench):
+    """The ours and reference lines build `config` from the same function and arguments."""
+    import inspect
+
+    src = inspect.getsource(bench.run_ours) + inspect.getsource(bench.run_reference)
+    assert src.count("workload_config(") == 2
+    fl = bench.WORKLOADS["batch_6m_1080_st"][4]
+    cfg = bench.workload_config("batch_6m_1080_st", 6_000_000, 1920, 1080, fl, 1, 1_440_000_000)
+    assert cfg["supersampling"] == 1 and cfg["use_gps"] is False and cfg["hybrid_scheduling"] is False
+    assert "larger than L2" in cfg["l2"]

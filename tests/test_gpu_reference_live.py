@@ -10,7 +10,7 @@ import torch
 
 import sgs_scenes
 from oracle import build_ref
-from sgs_testing import assert_bitwise, render_once
+from sgs_testing import assert_bitwise, reference_render, render_once
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not build_ref.available(), reason="reference oracle not built (oracle/build_ref.py)")]
@@ -126,9 +126,7 @@ def test_render_binding_progressive_live(ref, cuda_device):
                                   cam.focal_x, cam.focal_y, cam.center_x, cam.center_y, cam.near_plane, cam.far_plane,
                                   False, ss, gps, False, reuse, torch.empty(0, dtype=torch.uint8, device=dev), *kb, *h,
                                   v2pv.to(dev), mode)
-            frame = test_render_binding_progressive_live.ref_calls
-            h_ref = ref_C.render(*args(kb_ref, h_ref))
-            test_render_binding_progressive_live.ref_calls += 1
+            frame, h_ref = reference_render(ref_C, *args(kb_ref, h_ref))
             _C.set_frame_index(frame)
             h_our = _C.render(*args(kb_our, h_our))
             torch.cuda.synchronize()
@@ -138,5 +136,3 @@ def test_render_binding_progressive_live(ref, cuda_device):
                 assert_bitwise("k-buffer primitives", kb_our[0].cpu().numpy(), kb_ref[0].cpu().numpy())
             prev = cam
 
-
-test_render_binding_progressive_live.ref_calls = 0
