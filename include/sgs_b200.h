@@ -144,18 +144,30 @@ int sgs_render_split(const sgs_gaussians* gaussians, const sgs_camera* camera, c
 /* Several samples in one call (no counterpart in the reference; it is the sample loop of
  * Renderer.py:85-87 moved onto the device): renders n_samples samples with frame indices f .. f + n - 1
  * (f = the current frame index, which advances by n) and merges them into the history in order, the
- * first in settings->temporal_mode (Reset or Static) and the rest Static. The outputs equal those of
- * n_samples sgs_render calls bit for bit. Stochastic transparency: one walk over the Gaussians'
- * fragments evaluates each fragment's alpha once and every sample's threshold; GPS (scatter
- * scheduling): one projection, then each frame's point draws; one resolve pass reads the history
- * once. Not with spatial reuse, Reproject or hybrid GPS (SGS_ERROR_INVALID_ARGUMENT);
- * n_samples from 1 to 1024. The workspace holds sgs_samples_workspace_size(..., n_samples) bytes
- * (n_samples framebuffers). */
+ * first in settings->temporal_mode and the rest Static. The outputs (and, with spatial reuse, the
+ * k-buffer) equal those of n_samples sgs_render calls bit for bit. Stochastic transparency: one walk
+ * over the Gaussians' fragments evaluates each fragment's alpha once and every sample's threshold;
+ * GPS with scatter scheduling: one projection, then each frame's point draws; GPS with hybrid
+ * scheduling: each frame's scatter and queue passes into its own framebuffer; in these three cases one
+ * resolve pass reads the history once and merges the n framebuffers. With spatial reuse or a first
+ * sample in Reproject, the k-buffer and the reprojected history change sample by sample, so the
+ * whole pipeline runs once per sample inside the call. n_samples from 1 to 1024. The workspace holds
+ * sgs_samples_workspace_size(..., n_samples) bytes (n_samples framebuffers). */
 size_t sgs_samples_workspace_size(const sgs_gaussians* gaussians, const sgs_camera* camera,
                                   const sgs_settings* settings, uint32_t n_samples);
 int sgs_render_samples(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
                        const sgs_history* history, const sgs_outputs* outputs, uint32_t n_samples, void* workspace,
                        size_t workspace_bytes, void* stream);
+
+/* The frame compositing of the reference's renderer plugin (Renderer.py:91-97), on the device: for
+ * each of n_pixels pixels of a history (image (n, 3) premultiplied, depth and alpha (n)), alpha_out =
+ * clamp(alpha, 0, 1), rgb = clamp(image + (1 - alpha_out) * background_rgb, 0, 1) and depth_out =
+ * depth / max(alpha_out, 1e-8), each operation rounded like the separate elementwise tensor operations
+ * of the plugin (so the results equal them bit for bit). background_rgb is a device pointer to 3
+ * floats, so a captured CUDA graph reads the current background on every replay; depth_out and
+ * alpha_out may be NULL (depth may then be NULL too). */
+int sgs_composite(const float* image, const float* depth, const float* alpha, const float* background_rgb,
+                  uint32_t n_pixels, float* rgb, float* depth_out, float* alpha_out, void* stream);
 
 /* sgs_render for callers that cannot allocate device memory while rendering (a plugin inside a
  * host application under a fixed memory budget, a C caller without a caching allocator). It has no

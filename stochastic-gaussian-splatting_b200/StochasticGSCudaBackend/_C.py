@@ -115,6 +115,34 @@ def probe_atomic_min(slots: torch.Tensor, ops_per_thread: int, blocks: int, patt
     return int(blocks) * 256 * int(ops_per_thread)
 
 
+def composite(image: torch.Tensor, depth: torch.Tensor, alpha: torch.Tensor, background: torch.Tensor,
+              out: tuple | None = None):
+    """The renderer plugin's frame compositing (Renderer.py:91-97) as one kernel (sgs_composite) on the
+    current stream: returns (rgb, depth, alpha) = (clamp(image + (1 - a) * background, 0, 1),
+    depth / max(a, 1e-8), a) with a = clamp(alpha, 0, 1), bit for bit the values of those tensor
+    operations. `background` is a (3,) float32 CUDA tensor; `out` optionally three caller-owned tensors
+    of the result shapes (nothing is allocated then, so the call can sit in a CUDA graph)."""
+    device = image.device
+    image = _cuda_f32(image, "image", device)
+    depth = _cuda_f32(depth, "depth", device)
+    alpha = _cuda_f32(alpha, "alpha", device)
+    background = _cuda_f32(background, "background", device)
+    n = alpha.numel()
+    _check(image.numel() == 3 * n and depth.numel() == n and background.numel() == 3,
+           "image (H, W, 3), depth and alpha (H, W, 1) and a background of 3 values")
+    if out is None:
+        out = (torch.empty_like(image), torch.empty_like(depth), torch.empty_like(alpha))
+    for t, ref in zip(out, (image, depth, alpha)):
+        _check(t.is_cuda and t.device == device and t.dtype == torch.float32 and t.is_contiguous()
+               and t.numel() == ref.numel(), "outputs must be contiguous float32 tensors of the inputs' sizes")
+    stream = torch.cuda.current_stream(device).cuda_stream
+    status = _lib.sgs_composite(image.data_ptr(), depth.data_ptr(), alpha.data_ptr(), background.data_ptr(), n,
+                                out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), ctypes.c_void_p(stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_composite failed ({status}): {_abi.last_error(_lib)}")
+    return out
+
+
 def _check(cond: bool, msg: str) -> None:
     if not cond:
         raise RuntimeError(msg)
@@ -289,36 +317,37 @@ def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cud
                         preactivated=preactivated, caps=dict(max_fragments=max_fragments, max_binned=max_binned))
 
 
-def render_samples(n_samples: int, *args, preactivated=None):
+def render_samples(n_samples: int, *args, preactivated=None, **caps):
     """`n_samples` samples in one call (the C ABI's sgs_render_samples): the same 29 arguments as
-    `render`, frames f .. f + n_samples - 1 merged in order (the first in the given temporal mode,
-    Reset or Static, the rest Static); returns the final (image, depth, alpha, weight_mass), equal
-    bit for bit to `n_samples` `render` calls. No spatial reuse; GPS with scatter scheduling only."""
-    return _render_samples(n_samples, args, want_workspace=False, preactivated=preactivated)
+    `render`, frames f .. f + n_samples - 1 merged in order (the first in the given temporal mode, the
+    rest Static); returns the final (image, depth, alpha, weight_mass), equal bit for bit to
+    `n_samples` `render` calls (the k-buffer too, with spatial reuse). Keyword extras as `render`."""
+    return _render_samples(n_samples, args, want_workspace=False, preactivated=preactivated, caps=caps)
 
 
-def render_samples_with_workspace(n_samples: int, *args, preactivated=None):
+def render_samples_with_workspace(n_samples: int, *args, preactivated=None, **caps):
     """As `render_samples`, plus the workspace (its framebuffer section holds the n_samples winner
-    framebuffers back to back) and its layout."""
-    return _render_samples(n_samples, args, want_workspace=True, preactivated=preactivated)
+    framebuffers back to back; with spatial reuse or a Reproject first sample, only the last sample's
+    framebuffer, in the first slot) and its layout."""
+    return _render_samples(n_samples, args, want_workspace=True, preactivated=preactivated, caps=caps)
 
 
-def _render_samples(n_samples: int, args, want_workspace: bool, preactivated=None):
+def _render_samples(n_samples: int, args, want_workspace: bool, preactivated=None, caps=None):
     if len(args) != 29:
         raise TypeError(f"render_samples() takes n_samples and 29 render arguments ({len(args)} given)")
     n = int(n_samples)
     _check(1 <= n <= 1024, f"n_samples must be between 1 and 1024, got {n}")
+    caps = dict(caps or {})
+    _check(set(caps) <= {"max_fragments", "max_binned"}, f"unexpected keyword arguments {sorted(caps)}")
     device = args[0].device if isinstance(args[0], torch.Tensor) else None
     if device is not None and device.type == "cuda" and device.index != torch.cuda.current_device():
         with torch.cuda.device(device):
-            return _render_samples_impl(n, args, want_workspace, preactivated)
-    return _render_samples_impl(n, args, want_workspace, preactivated)
+            return _render_samples_impl(n, args, want_workspace, preactivated, caps)
+    return _render_samples_impl(n, args, want_workspace, preactivated, caps)
 
 
-def _render_samples_impl(n: int, args, want_workspace: bool, preactivated=None):
-    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated)
-    _check(not (s.use_gps and s.hybrid_scheduling) and not s.spatial_reuse and s.temporal_mode in (0, 1),
-           "render_samples needs no spatial reuse, Reset or Static mode, and for GPS scatter scheduling")
+def _render_samples_impl(n: int, args, want_workspace: bool, preactivated=None, caps=None):
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated, **(caps or {}))
     opts = dict(dtype=torch.float32, device=device)
     outs = (torch.empty((height, width, 3), **opts), torch.empty((height, width, 1), **opts),
             torch.empty((height, width, 1), **opts), torch.empty((height, width, 1), **opts))
@@ -382,6 +411,48 @@ def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=N
     if status != _abi.SGS_OK:
         raise RuntimeError(f"sgs_render_split failed ({status}): {_abi.last_error(_lib)}")
     del keep
+
+
+def render_samples_into(outputs, workspace: torch.Tensor, n_samples: int, *args, preactivated=None, max_fragments=0,
+                        max_binned=0) -> None:
+    """`render_samples` into caller-owned buffers: `outputs` = (image (H, W, 3), depth, alpha,
+    weight_mass (H, W, 1)) float32 CUDA tensors, not the history; `workspace` a uint8 CUDA tensor of
+    at least `samples_workspace_size(n_samples, *args)` bytes, 256-byte aligned. Nothing is allocated,
+    so the call can be captured in a CUDA graph."""
+    if len(args) != 29:
+        raise TypeError(f"render_samples_into() takes outputs, workspace, n_samples and 29 render arguments "
+                        f"({len(args)} given)")
+    n = int(n_samples)
+    _check(1 <= n <= 1024, f"n_samples must be between 1 and 1024, got {n}")
+    device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated, max_fragments=max_fragments,
+                                                         max_binned=max_binned)
+    shapes = ((height, width, 3), (height, width, 1), (height, width, 1), (height, width, 1))
+    for name, t, shape in zip(("image", "depth", "alpha", "weight_mass"), outputs, shapes):
+        _check(isinstance(t, torch.Tensor) and t.is_cuda and t.device == device and t.dtype == torch.float32
+               and tuple(t.shape) == shape and t.is_contiguous(),
+               f"output {name} must be a contiguous {shape} float32 CUDA tensor on {device}")
+    ws_bytes = int(_lib.sgs_samples_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), n))
+    _check(ws_bytes > 0, _abi.last_error(_lib) or "invalid render arguments")
+    _check(workspace.is_cuda and workspace.device == device and workspace.dtype == torch.uint8
+           and workspace.numel() >= ws_bytes and workspace.data_ptr() % 256 == 0,
+           f"workspace must be a 256-byte aligned uint8 CUDA tensor of at least {ws_bytes} bytes")
+    o = _abi.Outputs(*(t.data_ptr() for t in outputs))
+    stream = torch.cuda.current_stream(device).cuda_stream
+    status = _lib.sgs_render_samples(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.byref(h),
+                                     ctypes.byref(o), n, ctypes.c_void_p(workspace.data_ptr()),
+                                     ctypes.c_size_t(workspace.numel()), ctypes.c_void_p(stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_render_samples failed ({status}): {_abi.last_error(_lib)}")
+    del keep
+
+
+def samples_workspace_size(n_samples: int, *args, max_fragments=0, max_binned=0) -> int:
+    """Bytes of scratch `render_samples` with these 29 arguments needs (sgs_samples_workspace_size)."""
+    _, g, c, s, _, _, _ = _prepare(*args, max_fragments=max_fragments, max_binned=max_binned)
+    n = int(_lib.sgs_samples_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), int(n_samples)))
+    if n == 0:
+        raise RuntimeError(_abi.last_error(_lib) or "invalid render arguments")
+    return n
 
 
 def render_with_workspace(*args, preactivated=None, max_fragments=0, max_binned=0):

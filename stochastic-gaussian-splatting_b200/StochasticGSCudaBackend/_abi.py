@@ -114,6 +114,9 @@ SGS_CONV_MASK = 2
 
 # every entry point of include/sgs_b200.h: name -> (restype, argtypes)
 SIGNATURES = {
+    "sgs_composite": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
     "sgs_workspace_size": (ctypes.c_size_t, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera), ctypes.POINTER(SettingsC)]),
     "sgs_get_workspace_layout": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.POINTER(Camera),
                                                 ctypes.POINTER(SettingsC), ctypes.POINTER(WorkspaceLayout)]),

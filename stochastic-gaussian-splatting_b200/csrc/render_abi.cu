@@ -214,10 +214,8 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     if (st != SGS_OK) return st;
     if (n_samples == 0 || n_samples > kMaxSamplesPerCall)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "%u samples per call (1 to %u)", n_samples, kMaxSamplesPerCall);
-    if (n_samples > 1 && ((s->use_gps && s->hybrid_scheduling) || s->spatial_reuse ||
-                          s->temporal_mode == SGS_TEMPORAL_REPROJECT))
-        return fail(SGS_ERROR_INVALID_ARGUMENT,
-                    "several samples per call need no spatial reuse, Reset or Static, and for GPS scatter scheduling");
+    if (n_samples > 1 && acc_stream != res_stream)
+        return fail(SGS_ERROR_INVALID_ARGUMENT, "several samples per call run on one stream");
     if (static_cast<uint64_t>(d.n_fb) * n_samples > 0xffffffffull)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "the samples' framebuffers exceed 2^32 pixels");
     if (h == nullptr || o == nullptr) return fail(SGS_ERROR_INVALID_ARGUMENT, "null history or outputs");
@@ -256,7 +254,6 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
         t_split_event = nullptr;
         return fail(SGS_ERROR_CUDA, "could not create the event between the accumulate and resolve streams");
     }
-    cudaStream_t stream = acc_stream;
     char* ws = static_cast<char*>(workspace);
     // the host counter serves calls that keep no frame index in device memory
     const uint32_t frame =
@@ -275,37 +272,28 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     w.q.count = reinterpret_cast<uint32_t*>(ws + F.q_count);
     w.q.capacity = d.queue_capacity;
 
-    cudaError_t err = launch_clear(w.framebuffer, d.n_fb * n_samples, w.queue, sms, stream);
-    if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "clear: %s", cudaGetErrorString(err));
-
     const PassCamera cam = pass_camera(c, s, d.ss);
-    if (g->n_gaussians > 0) {
-        AccumulateParams ap{};
-        ap.means = g->means;
-        ap.scales = g->scales;
-        ap.rotations = reinterpret_cast<const float4*>(g->rotations);
-        ap.opacities = g->opacities;
-        ap.w2c = reinterpret_cast<const float4*>(c->w2c);
-        ap.framebuffer = w.framebuffer;
-        ap.n = g->n_gaussians;
-        ap.frame_idx = frame;
-        ap.frame_ptr = s->frame_index_device;
-        ap.cam = cam;
-        // the kernels pick one blue-noise slice per frame, rotated by the golden ratio per pass
-        ap.blue_noise = s->use_gps ? nullptr : s->blue_noise;
-        ap.max_fragments = s->max_fragments;
-        ap.max_binned = d.max_binned;
-        ap.hybrid = s->hybrid_scheduling != 0;
-        ap.queue = w.queue;
-        ap.q = w.q;
-        ap.n_samples = n_samples;
-        ap.fb_stride = d.n_fb;
-        ap.pre = reinterpret_cast<const float4*>(g->preactivated);
-        if (t_stage_start != nullptr) cudaEventRecord(t_stage_start, stream);
-        err = s->use_gps ? launch_accumulate_gps(ap, sms, stream) : launch_accumulate_st(ap, sms, stream);
-        if (t_stage_end != nullptr && err == cudaSuccess) err = cudaEventRecord(t_stage_end, stream);
-        if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "accumulate: %s", cudaGetErrorString(err));
-    }
+    AccumulateParams ap{};
+    ap.means = g->means;
+    ap.scales = g->scales;
+    ap.rotations = reinterpret_cast<const float4*>(g->rotations);
+    ap.opacities = g->opacities;
+    ap.w2c = reinterpret_cast<const float4*>(c->w2c);
+    ap.framebuffer = w.framebuffer;
+    ap.n = g->n_gaussians;
+    ap.frame_idx = frame;
+    ap.frame_ptr = s->frame_index_device;
+    ap.cam = cam;
+    // the kernels pick one blue-noise slice per frame, rotated by the golden ratio per pass
+    ap.blue_noise = s->use_gps ? nullptr : s->blue_noise;
+    ap.max_fragments = s->max_fragments;
+    ap.max_binned = d.max_binned;
+    ap.hybrid = s->hybrid_scheduling != 0;
+    ap.queue = w.queue;
+    ap.q = w.q;
+    ap.n_samples = n_samples;
+    ap.fb_stride = d.n_fb;
+    ap.pre = reinterpret_cast<const float4*>(g->preactivated);
 
     ResolveParams rp{};
     rp.means = g->means;
@@ -347,6 +335,73 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     rp.temporal_mode = s->temporal_mode;
     rp.n_samples = n_samples;
     rp.fb_stride = d.n_fb;
+
+    // the clear and accumulate passes of one framebuffer (or, with p.n_samples > 1, of all of them)
+    auto accumulate = [&](const AccumulateParams& p, const size_t n_clear) -> int {
+        cudaError_t err = launch_clear(p.framebuffer, n_clear, w.queue, sms, acc_stream);
+        if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "clear: %s", cudaGetErrorString(err));
+        if (g->n_gaussians == 0) return SGS_OK;
+        if (t_stage_start != nullptr) cudaEventRecord(t_stage_start, acc_stream);
+        err = s->use_gps ? launch_accumulate_gps(p, sms, acc_stream) : launch_accumulate_st(p, sms, acc_stream);
+        if (t_stage_end != nullptr && err == cudaSuccess) err = cudaEventRecord(t_stage_end, acc_stream);
+        if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "accumulate: %s", cudaGetErrorString(err));
+        return SGS_OK;
+    };
+    auto resolve = [&](const ResolveParams& r) -> int {
+        const cudaError_t err = launch_sample_resolve(r, res_stream);
+        if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));
+        return SGS_OK;
+    };
+
+    if (n_samples > 1 && (s->spatial_reuse || s->temporal_mode == SGS_TEMPORAL_REPROJECT)) {
+        // The k-buffer and the Reproject history are updated sample by sample: the whole pipeline runs
+        // once per sample, the first in the call's temporal mode and the rest Static, each merging into
+        // the outputs in place (a Static resolve reads a pixel's history only in the thread that writes
+        // the pixel). The same passes as n_samples single calls.
+        for (uint32_t sm = 0; sm < n_samples; ++sm) {
+            AccumulateParams pa = ap;
+            pa.n_samples = 1;
+            pa.frame_idx = frame + sm;
+            ResolveParams pr = rp;
+            pr.n_samples = 1;
+            if (sm > 0) {
+                pr.temporal_mode = SGS_TEMPORAL_STATIC;
+                pr.hist_image = o->image;
+                pr.hist_depth = o->depth;
+                pr.hist_alpha = o->alpha;
+                pr.hist_weight_mass = o->weight_mass;
+            }
+            st = accumulate(pa, d.n_fb);
+            if (st == SGS_OK) st = resolve(pr);
+            if (st != SGS_OK) return st;
+        }
+        return SGS_OK;
+    }
+    if (n_samples > 1 && s->use_gps && s->hybrid_scheduling) {
+        // Several GPS samples with hybrid scheduling: each frame's points are drawn by its own scatter
+        // and queue passes into its own framebuffer (the work queue is reused in stream order), then one
+        // resolve pass merges the n framebuffers in frame order.
+        cudaError_t err = launch_clear(w.framebuffer, d.n_fb * n_samples, w.queue, sms, acc_stream);
+        if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "clear: %s", cudaGetErrorString(err));
+        if (t_stage_start != nullptr) cudaEventRecord(t_stage_start, acc_stream);
+        for (uint32_t sm = 0; sm < n_samples && g->n_gaussians > 0; ++sm) {
+            AccumulateParams pa = ap;
+            pa.n_samples = 1;
+            pa.framebuffer = w.framebuffer + static_cast<size_t>(sm) * d.n_fb;
+            pa.frame_offset = sm;
+            if (sm > 0) {
+                err = launch_clear(pa.framebuffer, 0, w.queue, sms, acc_stream);  // the queue header only
+                if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "clear: %s", cudaGetErrorString(err));
+            }
+            err = launch_accumulate_gps(pa, sms, acc_stream);
+            if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "accumulate: %s", cudaGetErrorString(err));
+        }
+        if (t_stage_end != nullptr) cudaEventRecord(t_stage_end, acc_stream);
+        return resolve(rp);
+    }
+
+    st = accumulate(ap, d.n_fb * n_samples);
+    if (st != SGS_OK) return st;
     if (split) {
         // the next call's accumulate pass may start before this resolve: advance the device-resident
         // frame index behind this accumulate pass instead
@@ -354,14 +409,12 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
             advance_frame_kernel<<<1, 1, 0, acc_stream>>>(s->frame_index_device, n_samples);
             rp.frame_counter = nullptr;
         }
-        err = cudaEventRecord(t_split_event, acc_stream);
+        cudaError_t err = cudaEventRecord(t_split_event, acc_stream);
         if (err == cudaSuccess) err = cudaStreamWaitEvent(res_stream, t_split_event, 0);
         if (err == cudaSuccess) err = cudaGetLastError();
         if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "stream split: %s", cudaGetErrorString(err));
     }
-    err = launch_sample_resolve(rp, res_stream);
-    if (err != cudaSuccess) return fail(SGS_ERROR_CUDA, "sample/resolve: %s", cudaGetErrorString(err));
-    return SGS_OK;
+    return resolve(rp);
 }
 
 }  // namespace

@@ -74,6 +74,7 @@ struct AccumulateParams {
     uint32_t n;
     uint32_t frame_idx;               // used when frame_ptr is null
     const uint32_t* frame_ptr;        // device-resident frame index, or null
+    uint32_t frame_offset;            // added to either: sample s of a call whose passes run per sample
     PassCamera cam;
     const uint8_t* blue_noise;        // (64, 128, 128) volume; null: white noise
     uint32_t max_fragments;           // GPS point cap per Gaussian
@@ -106,13 +107,15 @@ __device__ __forceinline__ FrameRng frame_rng_at(const AccumulateParams& a, cons
 }
 
 __device__ __forceinline__ FrameRng frame_rng(const AccumulateParams& a) {
-    return frame_rng_at(a, a.frame_ptr != nullptr ? *a.frame_ptr : a.frame_idx);
+    return frame_rng_at(a, (a.frame_ptr != nullptr ? *a.frame_ptr : a.frame_idx) + a.frame_offset);
 }
 
 cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue* queue, int num_sms,
                          cudaStream_t stream);
 cudaError_t launch_accumulate_st(const AccumulateParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_composite(const float* image, const float* depth, const float* alpha, const float* background,
+                             uint32_t n, float* rgb, float* depth_out, float* alpha_out, cudaStream_t stream);
 cudaError_t launch_preactivate(const float* scales, const float4* rotations, const float* opacities, uint32_t n,
                               float4* out, cudaStream_t stream);
 cudaError_t launch_atomic_min_probe(unsigned long long* slots, uint64_t n_slots, uint32_t ops, uint32_t blocks,

@@ -8,8 +8,10 @@ available here. This module restates what those callers do, on this library:
   the pose changed or progressive rendering is disabled; STATIC when the pose is unchanged; otherwise
   REPROJECT with temporal reuse, else RESET; SAMPLES_PER_PIXEL samples, the first in that mode and
   the rest STATIC; then the background composite and the depth normalisation. The sample loop runs
-  as one `_C.render_samples` call where that path applies (no spatial reuse, first mode RESET or
-  STATIC, GPS only with scatter scheduling), which renders the same bits as the loop.
+  as one `_C.render_samples` call, which renders the same bits as the loop in every mode. With
+  `graphs=True` every frame is one CUDA graph launch: the pose, background and frame index are copied
+  in from pinned host memory, the samples rendered and the frame composited (`_C.composite`) by the
+  replayed graph of the frame's temporal mode, with the same bits as the eager frame.
 * `load_camera_path(path)` reads the camera-path .json of Trainer.py:28-65 (per frame: `rotation`
   3x3 and `position` of camera-to-world, `fx`, `fy`, `width`, `height`, `id`).
 * `benchmark_camera_path(renderer, views)` is the FPS measurement of Trainer.py:79-120: one warm-up
@@ -81,7 +83,8 @@ class ProgressiveRenderer:
     def __init__(self, means, scales, rotations, opacities, sh_coefficients, *, proper_antialiasing: bool = False,
                  use_gps: bool = False, hybrid_scheduling: bool = False, supersampling_factor: int = 1,
                  samples_per_pixel: int = 1, disable_progressive_rendering: bool = False,
-                 spatial_reuse: bool = False, temporal_reuse: bool = False, preactivate: bool = False):
+                 spatial_reuse: bool = False, temporal_reuse: bool = False, preactivate: bool = False,
+                 graphs: bool = False):
         self.model = (means, scales, rotations, opacities, sh_coefficients)
         # covariance and opacity sigmoid once per model (README.md:139-142); the images are the same bits
         self.preactivated = _C.preactivate(scales, rotations, opacities) if preactivate else None
@@ -99,6 +102,8 @@ class ProgressiveRenderer:
         self.history = None
         self.history_c2w = None
         self.history_w2c = None
+        self.graphs = graphs
+        self._frames = None  # _FrameGraphs of the current settings (graphs=True)
 
     def _settings(self, view: View) -> Settings:
         w2c, pos, _ = view.pose(self.device)
@@ -112,43 +117,52 @@ class ProgressiveRenderer:
         return a.as_tuple()[2:] == b.as_tuple()[2:]
 
     def _samples(self, settings: Settings, v2pv: torch.Tensor, mode: TemporalMode, n: int) -> None:
-        """n samples merged into the history, the first in `mode`, the rest STATIC."""
-        one_call = (not (settings.use_gps and settings.hybrid_scheduling) and not settings.spatial_reuse
-                    and mode in (TemporalMode.RESET, TemporalMode.STATIC) and n > 1)
-        if one_call:
-            self.history = History(*_C.render_samples(
-                n, *self.model, *settings.as_tuple(), _blue_noise(self.device), *self.k_buffer, *self.history, v2pv,
-                int(mode), preactivated=self.preactivated))
-            return
-        for _ in range(n):
-            self.history = render(*self.model, settings, self.k_buffer, self.history, v2pv, mode,
-                                  preactivated=self.preactivated)
-            mode = TemporalMode.STATIC
+        """n samples merged into the history, the first in `mode`, the rest STATIC (one call)."""
+        self.history = History(*_C.render_samples(
+            n, *self.model, *settings.as_tuple(), _blue_noise(self.device), *self.k_buffer, *self.history, v2pv,
+            int(mode), preactivated=self.preactivated))
+
+    def _frame_mode(self, view: View, settings: Settings, benchmark: bool) -> TemporalMode:
+        """The temporal mode of the frame's first sample (Renderer.py:73-84); a new k-buffer and an empty
+        history when any setting but the pose changed."""
+        reset = self.disable_progressive_rendering and not benchmark
+        changed = self.settings is None or not self._same_settings(settings, self.settings)
+        if reset or changed:
+            self.settings = settings
+            if changed or not self.graphs:
+                self.k_buffer = create_k_buffer(settings)
+                self._frames = None
+            else:
+                # the captured graphs keep this k-buffer: emptied in place (entries -1, as created)
+                self.k_buffer[0].fill_(-1)
+            self.history = History(*(torch.empty(0) for _ in range(4)))
+            return TemporalMode.RESET
+        if (self.history_c2w == view.c2w).all():
+            return TemporalMode.STATIC
+        return TemporalMode.REPROJECT if self.temporal_reuse else TemporalMode.RESET
 
     @torch.inference_mode()
     def render_image(self, view: View, to_chw: bool = False, benchmark: bool = False) -> dict[str, torch.Tensor]:
         settings = self._settings(view)
-        reset = self.disable_progressive_rendering and not benchmark
-        if reset or self.settings is None or not self._same_settings(settings, self.settings):
-            self.settings = settings
-            self.k_buffer = create_k_buffer(settings)
-            self.history = History(*(torch.empty(0) for _ in range(4)))
-            mode = TemporalMode.RESET
-        elif (self.history_c2w == view.c2w).all():
-            mode = TemporalMode.STATIC
-        else:
-            mode = TemporalMode.REPROJECT if self.temporal_reuse else TemporalMode.RESET
-        _, _, c2w = view.pose(self.device)
-        v2pv = self.history_w2c @ c2w if mode == TemporalMode.REPROJECT else c2w
+        mode = self._frame_mode(view, settings, benchmark)
         n = max(self.samples_per_pixel, 1)
-        if mode == TemporalMode.REPROJECT:
-            self._samples(settings, v2pv, mode, 1)
-            n -= 1
-            mode = TemporalMode.STATIC
-        if n > 0:
+        if self.graphs:
+            if self._frames is None:
+                self._frames = _FrameGraphs(self, settings, n)
+            image, depth, alpha = self._frames.frame(view, self.history_c2w, mode)
+            self.history = self._frames.history()
+        else:
+            _, _, c2w = view.pose(self.device)
+            v2pv = self.history_w2c @ c2w if mode == TemporalMode.REPROJECT else c2w
             self._samples(settings, v2pv, mode, n)
         self.history_c2w = view.c2w.copy()
         self.history_w2c = view.pose(self.device)[0]
+        if self.graphs:
+            if benchmark:
+                return {"rgb": image}
+            if to_chw:
+                image, depth, alpha = image.permute(2, 0, 1), depth.permute(2, 0, 1), alpha.permute(2, 0, 1)
+            return {"rgb": image, "depth": depth, "alpha": alpha}
 
         # the history is premultiplied by alpha and must not be modified in place
         image, depth, alpha, _ = self.history
@@ -161,6 +175,116 @@ class ProgressiveRenderer:
         if to_chw:
             image, depth, alpha = image.permute(2, 0, 1), depth.permute(2, 0, 1), alpha.permute(2, 0, 1)
         return {"rgb": image, "depth": depth, "alpha": alpha}
+
+
+class _FrameGraphs:
+    """One CUDA graph per (temporal mode of the first sample, parity) for the frames of fixed settings.
+
+    A replayed graph copies the frame's parameters (w2c, camera position, the previous view's w2c, the
+    camera-to-world matrix, background, frame index) from a pinned host staging buffer into device
+    buffers, forms view-to-previous-view as the eager frame does (a float32 product on the GPU),
+    renders the frame's samples with `_C.render_samples_into` (frame index read from device memory)
+    from history buffer `parity` into history buffer 1 - parity, and composites the result into fixed
+    output buffers (`_C.composite`). Staging buffers alternate with the parity; a frame waits for the
+    replay two frames back (the same staging buffer) before writing its parameters. The output tensors
+    are overwritten by the next frame.
+    """
+
+    # w2c 16, position 3 (+1), previous w2c 16, c2w 16, background 3 (+1)
+    _W2C, _POS, _PREV, _C2W, _BG, _PARAMS = 0, 16, 20, 36, 52, 56
+
+    def __init__(self, renderer: "ProgressiveRenderer", settings: Settings, n_samples: int):
+        dev = renderer.device
+        self.r = renderer
+        self.n = n_samples
+        self.settings = settings
+        h, w = settings.height, settings.width
+        opts = dict(dtype=torch.float32, device=dev)
+        self.params = torch.zeros(self._PARAMS, **opts)
+        self.v2pv = torch.zeros((4, 4), **opts)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.staging = [torch.zeros(self._PARAMS, dtype=torch.float32).pin_memory() for _ in range(2)]
+        self.staging_frame = [torch.zeros(1, dtype=torch.int32).pin_memory() for _ in range(2)]
+        self.done = [torch.cuda.Event() for _ in range(2)]
+        self.used = [False, False]
+        self.hist = [tuple(torch.zeros(shape, **opts) for shape in ((h, w, 3), (h, w, 1), (h, w, 1), (h, w, 1)))
+                     for _ in range(2)]
+        self.out = (torch.empty((h, w, 3), **opts), torch.empty((h, w, 1), **opts), torch.empty((h, w, 1), **opts))
+        self.parity = 0
+        self.graphs = {}
+        self.workspace = None
+
+    def _param(self, at: int, n: int) -> torch.Tensor:
+        return self.params[at:at + n]
+
+    def _args(self, mode: TemporalMode, history, k_buffer):
+        s = self.settings
+        w2c = self._param(self._W2C, 16).view(4, 4)
+        pos = self._param(self._POS, 3)
+        e = torch.empty(0)
+        hist = history if mode != TemporalMode.RESET else (e, e, e, e)
+        v2pv = self.v2pv if mode == TemporalMode.REPROJECT else self._param(self._C2W, 16).view(4, 4)
+        return (*self.r.model, w2c, pos, *s.as_tuple()[2:], _blue_noise(self.r.device), *k_buffer, *hist, v2pv,
+                int(mode))
+
+    def _body(self, mode: TemporalMode, parity: int, k_buffer):
+        src, dst = self.hist[parity], self.hist[1 - parity]
+        if mode == TemporalMode.REPROJECT:
+            torch.matmul(self._param(self._PREV, 16).view(4, 4), self._param(self._C2W, 16).view(4, 4), out=self.v2pv)
+        _C.render_samples_into(dst, self.workspace, self.n, *self._args(mode, src, k_buffer),
+                               preactivated=self.r.preactivated)
+        _C.composite(dst[0], dst[1], dst[2], self._param(self._BG, 3), out=self.out)
+
+    def _capture(self, mode: TemporalMode, parity: int):
+        k_buffer = self.r.k_buffer
+        if self.workspace is None:
+            size = _C.samples_workspace_size(self.n, *self._args(mode, self.hist[parity], k_buffer))
+            raw = torch.empty(size + 256, dtype=torch.uint8, device=self.r.device)
+            off = (-raw.data_ptr()) % 256
+            self.workspace = raw[off:off + size]
+        _C.set_device_frame_counter(self.counter)
+        try:
+            # one uncaptured run of the same launches first (its scratch k-buffer keeps the real one intact;
+            # the staging copy at every replay restores the parameters and the frame index)
+            self.params.copy_(self.staging[parity])
+            scratch = tuple(t.clone() for t in k_buffer)
+            self._body(mode, parity, scratch)
+            torch.cuda.synchronize(self.r.device)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                self.params.copy_(self.staging[parity], non_blocking=True)
+                self.counter.copy_(self.staging_frame[parity], non_blocking=True)
+                self._body(mode, parity, k_buffer)
+        finally:
+            _C.set_device_frame_counter(None, self.r.device)
+        return graph
+
+    def frame(self, view: View, previous_c2w, mode: TemporalMode):
+        p = self.parity
+        if self.used[p]:
+            self.done[p].synchronize()
+        st = self.staging[p].numpy()
+        st[self._W2C:self._W2C + 16] = view.w2c_numpy.astype(np.float32).reshape(-1)
+        st[self._POS:self._POS + 3] = view.c2w[:3, 3].astype(np.float32)
+        if previous_c2w is not None:
+            st[self._PREV:self._PREV + 16] = np.linalg.inv(previous_c2w).astype(np.float32).reshape(-1)
+        st[self._C2W:self._C2W + 16] = view.c2w.astype(np.float32).reshape(-1)
+        st[self._BG:self._BG + 3] = np.asarray(view.background_color, dtype=np.float32)
+        frame = _C.get_frame_index()
+        self.staging_frame[p].numpy()[0] = np.uint32(frame).view(np.int32)
+        key = (int(mode), p)
+        if key not in self.graphs:
+            self.graphs[key] = self._capture(mode, p)
+        self.graphs[key].replay()
+        self.done[p].record()
+        self.used[p] = True
+        _C.set_frame_index(frame + self.n)
+        self.parity = 1 - p
+        return self.out
+
+    def history(self) -> History:
+        """The history the last frame wrote (the next frame's input)."""
+        return History(*self.hist[self.parity])
 
 
 def _blue_noise(device) -> torch.Tensor:

@@ -59,22 +59,44 @@ def _views(sgs_viewer):
 @pytest.mark.parametrize("flags", [dict(), dict(temporal_reuse=True), dict(temporal_reuse=True, spatial_reuse=True),
                                    dict(supersampling_factor=2, hybrid_scheduling=True),
                                    dict(use_gps=True, temporal_reuse=True), dict(preactivate=True),
-                                   dict(use_gps=True, temporal_reuse=True, spatial_reuse=True, preactivate=True)])
+                                   dict(use_gps=True, temporal_reuse=True, spatial_reuse=True, preactivate=True),
+                                   dict(use_gps=True, hybrid_scheduling=True, supersampling_factor=2,
+                                        temporal_reuse=True, spatial_reuse=True)])
 @pytest.mark.parametrize("spp", [1, 4])
-def test_progressive_renderer_equals_the_sample_loop(flags, spp, cuda_device):
+@pytest.mark.parametrize("graphs", [False, True])
+def test_progressive_renderer_equals_the_sample_loop(flags, spp, graphs, cuda_device):
+    """Eager frames (one render_samples call each) and replayed CUDA graphs (one launch per frame)."""
     import sgs_viewer
 
     scene = sgs_scenes.make_scene(sgs_scenes.SceneSpec(n=20_000, log_scale_mean=-3.5), seed=9)
     model = tuple(t.cuda() for t in scene.tensors())
-    ours = sgs_viewer.ProgressiveRenderer(*model, samples_per_pixel=spp, **flags)
+    ours = sgs_viewer.ProgressiveRenderer(*model, samples_per_pixel=spp, graphs=graphs, **flags)
     ref = LoopRenderer(model, spp, **flags)
     _C.set_frame_index(1000)
-    a = [ours.render_image(v) for v in _views(sgs_viewer)]
+    # graph frames are written into fixed buffers that the next frame overwrites
+    a = [{k: t.clone() for k, t in ours.render_image(v).items()} for v in _views(sgs_viewer)]
     _C.set_frame_index(1000)
     b = [ref.render_image(v) for v in _views(sgs_viewer)]
     for i, (x, y) in enumerate(zip(a, b)):
         for k in ("rgb", "depth", "alpha"):
             assert torch.equal(x[k], y[k]), f"frame {i} {k}"
+
+
+def test_composite_equals_the_tensor_operations(cuda_device):
+    """_C.composite (one kernel) against the plugin's tensor operations (Renderer.py:91-97), bit for bit,
+    with alphas below 0, above 1 and at 0."""
+    g = torch.Generator(device="cuda").manual_seed(4)
+    h, w = 37, 53
+    image = torch.rand((h, w, 3), device="cuda", generator=g) * 1.3 - 0.1
+    depth = torch.rand((h, w, 1), device="cuda", generator=g) * 20.0
+    alpha = torch.rand((h, w, 1), device="cuda", generator=g) * 1.4 - 0.2
+    alpha[0, :5] = 0.0
+    bg = torch.tensor([0.2, 0.7, 1.0], device="cuda")
+    rgb, d, a = _C.composite(image, depth, alpha, bg)
+    a_want = alpha.clamp(0.0, 1.0)
+    assert torch.equal(a, a_want)
+    assert torch.equal(rgb, (image + (1.0 - a_want) * bg).clamp(0.0, 1.0))
+    assert torch.equal(d, depth / a_want.clamp_min(1.0e-8))
 
 
 def test_camera_path_benchmark_and_png(tmp_path, cuda_device):
