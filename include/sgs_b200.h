@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define SGS_ABI_VERSION 3
+#define SGS_ABI_VERSION 4
 #define SGS_K_BUFFER_SIZE 4 /* k-buffer entries per (sub)pixel, resolve.h:9 / render.cu:164 */
 
 enum sgs_status {
@@ -52,6 +52,12 @@ typedef struct sgs_gaussians {
                                    * set, the accumulate pass reads covariance and opacity from it (the
                                    * same bits) instead of rebuilding them from scales, rotations and
                                    * opacities. It must match those arrays; nothing checks that. */
+    const void* quantized;        /* optional (N, 4) uint32 records of sgs_quantize, 16-byte aligned, or NULL;
+                                   * when set, every pass reads positions, rotations, scales and opacities
+                                   * from them (the float32 arrays above may then be NULL) */
+    const float* quantized_chunks; /* with `quantized`: the (sgs_quantized_chunks(N), 8) chunk table */
+    const void* sh_half;          /* with `quantized`: the (N, B, 3) IEEE half SH coefficients of sgs_quantize,
+                                   * read by the sample pass instead of sh_coefficients */
 } sgs_gaussians;
 
 /* Pinhole camera in image pixels (render.cu:22-31, render_utils.h:19-30). */
@@ -333,6 +339,19 @@ void sgs_set_queue_limit(uint32_t max_entries);
  * quaternion is usable (else 0). Computed once per model and passed as
  * sgs_gaussians.preactivated, it saves the per-sample rebuild; renders stay bit-identical. */
 int sgs_preactivate(const sgs_gaussians* gaussians, float* out, void* stream);
+
+/* Quantised layout (README.md:143-147 of the reference lists it as a possible improvement): encodes
+ * the Gaussians of `gaussians` (means, scales, rotations, opacities and, when sh_half is not NULL,
+ * sh_coefficients are read) into `records` ((N, 4) uint32, 16 bytes per Gaussian instead of 44:
+ * position in 11-10-11 bits inside the box of its chunk of 256 consecutive Gaussians, rotation as the
+ * three smallest components of the normalised quaternion in 10 bits each, log-scales and opacity
+ * logit as IEEE half), `chunks` ((sgs_quantized_chunks(N), 8) floats: each chunk's lower corner and
+ * extent) and `sh_half` ((N, B, 3) IEEE half). All three 16-byte aligned device memory. Passed as
+ * sgs_gaussians.quantized / quantized_chunks / sh_half, they replace the float32 arrays in every pass;
+ * the images then differ from the float32 ones by the quantisation (not bit-identical). Not usable with
+ * the backward. Morton-ordered Gaussians (as Model.py loads them) keep the chunks small. */
+uint32_t sgs_quantized_chunks(uint32_t n_gaussians);
+int sgs_quantize(const sgs_gaussians* gaussians, void* records, float* chunks, void* sh_half, void* stream);
 
 /* Measurement aid without a counterpart in the reference: launches `blocks` blocks of 256 threads,
  * each thread issuing `ops_per_thread` 64-bit atomic minimum reductions (red.min.u64, the merge of

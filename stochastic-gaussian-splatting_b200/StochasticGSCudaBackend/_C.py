@@ -101,6 +101,54 @@ def preactivate(scales: torch.Tensor, rotations: torch.Tensor, opacities: torch.
     return out
 
 
+class Quantized(tuple):
+    """The quantised layout of a model (`quantize`): (records (N, 4) int32, chunks (C, 8) float32,
+    sh_half (N, B, 3) float16)."""
+
+    __slots__ = ()
+
+    def __new__(cls, records, chunks, sh_half):
+        return super().__new__(cls, (records, chunks, sh_half))
+
+    records = property(lambda self: self[0])
+    chunks = property(lambda self: self[1])
+    sh_half = property(lambda self: self[2])
+
+    def nbytes(self) -> int:
+        return sum(t.numel() * t.element_size() for t in self)
+
+
+def quantize(means: torch.Tensor, scales: torch.Tensor, rotations: torch.Tensor, opacities: torch.Tensor,
+             sh_coefficients: torch.Tensor) -> Quantized:
+    """The quantised layout of these Gaussians (sgs_quantize): 16 bytes per Gaussian for positions (11-10-11
+    bits inside the box of each chunk of 256 consecutive Gaussians), rotations (three smallest quaternion
+    components, 10 bits each), log-scales and opacity logits (half), plus half-precision SH. Pass it as
+    `quantized=` to the render calls; the images then differ from the float32 ones by the quantisation.
+    Recompute it whenever the parameters change."""
+    device = means.device
+    means = _cuda_f32(means, "means", device)
+    scales = _cuda_f32(scales, "scales", device)
+    rotations = _cuda_f32(rotations, "rotations", device)
+    opacities = _cuda_f32(opacities, "opacities", device)
+    sh_coefficients = _cuda_f32(sh_coefficients, "sh_coefficients", device)
+    n = means.shape[0]
+    bases = sh_coefficients.shape[1]
+    _check(tuple(means.shape) == (n, 3) and tuple(scales.shape) == (n, 3) and tuple(rotations.shape) == (n, 4)
+           and opacities.numel() == n and tuple(sh_coefficients.shape) == (n, bases, 3) and bases in _VALID_SH_BASES,
+           "means (N, 3), scales (N, 3), rotations (N, 4), opacities (N) and sh_coefficients (N, B, 3)")
+    records = torch.empty((n, 4), dtype=torch.int32, device=device)
+    chunks = torch.empty((int(_lib.sgs_quantized_chunks(n)), 8), dtype=torch.float32, device=device)
+    sh_half = torch.empty((n, bases, 3), dtype=torch.float16, device=device)
+    g = _abi.Gaussians(_ptr(means), _ptr(scales), _ptr(rotations), _ptr(opacities), _ptr(sh_coefficients), n, bases)
+    with torch.cuda.device(device):
+        stream = torch.cuda.current_stream(device).cuda_stream
+        status = _lib.sgs_quantize(ctypes.byref(g), _ptr(records), _ptr(chunks), _ptr(sh_half),
+                                   ctypes.c_void_p(stream))
+    if status != _abi.SGS_OK:
+        raise RuntimeError(f"sgs_quantize failed ({status}): {_abi.last_error(_lib)}")
+    return Quantized(records, chunks, sh_half)
+
+
 def probe_atomic_min(slots: torch.Tensor, ops_per_thread: int, blocks: int, pattern: int = 0, seed: int = 0) -> int:
     """Launches the red.min.u64 throughput probe (sgs_probe_atomic_min) on the current stream into
     `slots` (a contiguous int64 CUDA tensor of power-of-two length); returns the number of
@@ -163,7 +211,7 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
              center_x, center_y, near_plane, far_plane, proper_antialiasing, supersampling_factor_raw, use_gps,
              hybrid_scheduling, spatial_reuse, blue_noise, k_buffer_primitives, k_buffer_occlusion, history_image,
              history_depth, history_alpha, history_weight_mass, view_to_previous_view, temporal_mode, preactivated=None,
-             max_fragments=0, max_binned=0):
+             max_fragments=0, max_binned=0, quantized=None):
     _check(isinstance(means, torch.Tensor) and means.is_cuda, "means must be a CUDA tensor")
     device = means.device
     means = _cuda_f32(means, "means", device)
@@ -228,8 +276,16 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
     max_fragments, max_binned = int(max_fragments or 0), int(max_binned or 0)
     _check(0 <= max_fragments < 2 ** 32 and 0 <= max_binned < 2 ** 32,
            "max_fragments and max_binned must be non-negative 32-bit counts (0 = the reference's default)")
+    if quantized is not None:
+        _check(isinstance(quantized, Quantized) and preactivated is None,
+               "quantized must be the result of quantize(), without preactivated=")
+        rec, chunks, sh_half = quantized
+        _check(rec.is_cuda and rec.device == device and tuple(rec.shape) == (n, 4) and rec.dtype == torch.int32
+               and tuple(sh_half.shape) == (n, sh_bases, 3) and sh_half.dtype == torch.float16
+               and chunks.shape[0] == int(_lib.sgs_quantized_chunks(n)),
+               "quantized does not describe these Gaussians")
     g = _abi.Gaussians(_ptr(means), _ptr(scales), _ptr(rotations), _ptr(opacities), _ptr(sh_coefficients), n, sh_bases,
-                       _ptr(preactivated))
+                       _ptr(preactivated), *((_ptr(t) for t in quantized) if quantized is not None else (None,) * 3))
     c = _abi.Camera(w2c.data_ptr(), cam_position.data_ptr(), width, height, float(focal_x), float(focal_y),
                     float(center_x), float(center_y), float(near_plane), float(far_plane))
     s = _abi.SettingsC(int(bool(proper_antialiasing)), ss, int(bool(use_gps)), int(bool(hybrid_scheduling)),
@@ -241,7 +297,7 @@ def _prepare(means, scales, rotations, opacities, sh_coefficients, w2c, cam_posi
         _ptr(k_buffer_primitives) if spatial_reuse else None, _ptr(k_buffer_occlusion) if spatial_reuse else None)
     # keep the contiguous copies alive for the duration of the call
     keep = (means, scales, rotations, opacities, sh_coefficients, w2c, cam_position, blue_noise, view_to_previous_view,
-            preactivated)
+            preactivated, *(quantized or ()))
     return device, g, c, s, h, (width, height), keep
 
 
@@ -288,7 +344,7 @@ def _render_impl(args, want_workspace: bool, streams=None, preactivated=None, ca
         return (image, depth, alpha, weight_mass), workspace, layout
 
 
-def render(*args, preactivated=None, max_fragments=0, max_binned=0):
+def render(*args, preactivated=None, max_fragments=0, max_binned=0, quantized=None):
     """`_C.render` with the reference's 29 positional arguments; returns (image, depth, alpha, weight_mass).
 
     Keyword-only extras (not in the reference's binding):
@@ -298,11 +354,13 @@ def render(*args, preactivated=None, max_fragments=0, max_binned=0):
                      round(W_fb * H_fb / (2 ss^2)), accumulate_hybrid_gps.cu:86);
       max_binned     capacity of the hybrid work queue in Gaussians (0: the reference's min(N, 2^20),
                      accumulate_hybrid_gps.cu:22 and accumulate_hybrid.cu:27). Gaussians beyond it are
-                     rendered in place, as in the reference."""
+                     rendered in place, as in the reference;
+      quantized      the `quantize()` layout of these Gaussians, read by every pass in place of the
+                     float32 arrays (the images differ by the quantisation)."""
     if len(args) != 29:
         raise TypeError(f"render() takes 29 positional arguments ({len(args)} given)")
     return _render_impl(args, want_workspace=False, preactivated=preactivated,
-                        caps=dict(max_fragments=max_fragments, max_binned=max_binned))
+                        caps=dict(max_fragments=max_fragments, max_binned=max_binned, quantized=quantized))
 
 
 def render_split(accumulate_stream: torch.cuda.Stream, resolve_stream: torch.cuda.Stream, *args, preactivated=None,
@@ -338,7 +396,7 @@ def _render_samples(n_samples: int, args, want_workspace: bool, preactivated=Non
     n = int(n_samples)
     _check(1 <= n <= 1024, f"n_samples must be between 1 and 1024, got {n}")
     caps = dict(caps or {})
-    _check(set(caps) <= {"max_fragments", "max_binned"}, f"unexpected keyword arguments {sorted(caps)}")
+    _check(set(caps) <= {"max_fragments", "max_binned", "quantized"}, f"unexpected keyword arguments {sorted(caps)}")
     device = args[0].device if isinstance(args[0], torch.Tensor) else None
     if device is not None and device.type == "cuda" and device.index != torch.cuda.current_device():
         with torch.cuda.device(device):
@@ -414,7 +472,7 @@ def render_into(outputs, workspace: torch.Tensor, streams, *args, preactivated=N
 
 
 def render_samples_into(outputs, workspace: torch.Tensor, n_samples: int, *args, preactivated=None, max_fragments=0,
-                        max_binned=0) -> None:
+                        max_binned=0, quantized=None) -> None:
     """`render_samples` into caller-owned buffers: `outputs` = (image (H, W, 3), depth, alpha,
     weight_mass (H, W, 1)) float32 CUDA tensors, not the history; `workspace` a uint8 CUDA tensor of
     at least `samples_workspace_size(n_samples, *args)` bytes, 256-byte aligned. Nothing is allocated,
@@ -425,7 +483,7 @@ def render_samples_into(outputs, workspace: torch.Tensor, n_samples: int, *args,
     n = int(n_samples)
     _check(1 <= n <= 1024, f"n_samples must be between 1 and 1024, got {n}")
     device, g, c, s, h, (width, height), keep = _prepare(*args, preactivated=preactivated, max_fragments=max_fragments,
-                                                         max_binned=max_binned)
+                                                         max_binned=max_binned, quantized=quantized)
     shapes = ((height, width, 3), (height, width, 1), (height, width, 1), (height, width, 1))
     for name, t, shape in zip(("image", "depth", "alpha", "weight_mass"), outputs, shapes):
         _check(isinstance(t, torch.Tensor) and t.is_cuda and t.device == device and t.dtype == torch.float32
@@ -455,12 +513,12 @@ def samples_workspace_size(n_samples: int, *args, max_fragments=0, max_binned=0)
     return n
 
 
-def render_with_workspace(*args, preactivated=None, max_fragments=0, max_binned=0):
+def render_with_workspace(*args, preactivated=None, max_fragments=0, max_binned=0, quantized=None):
     """As `render`, plus the workspace tensor and its layout (winner framebuffer, samples, reuse weights)."""
     if len(args) != 29:
         raise TypeError(f"render_with_workspace() takes 29 positional arguments ({len(args)} given)")
     return _render_impl(args, want_workspace=True, preactivated=preactivated,
-                        caps=dict(max_fragments=max_fragments, max_binned=max_binned))
+                        caps=dict(max_fragments=max_fragments, max_binned=max_binned, quantized=quantized))
 
 
 def workspace_views(workspace: torch.Tensor, layout, n_fb: int, spatial_reuse: bool) -> dict[str, torch.Tensor]:

@@ -9,7 +9,7 @@ import ctypes
 from pathlib import Path
 
 LIB_NAME = "libsgs_b200.so"
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 SGS_OK = 0
 SGS_ERROR_INVALID_ARGUMENT = -1
@@ -27,6 +27,9 @@ class Gaussians(ctypes.Structure):
         ("n_gaussians", ctypes.c_uint32),
         ("sh_bases", ctypes.c_uint32),
         ("preactivated", ctypes.c_void_p),
+        ("quantized", ctypes.c_void_p),
+        ("quantized_chunks", ctypes.c_void_p),
+        ("sh_half", ctypes.c_void_p),
     ]
 
 
@@ -114,6 +117,9 @@ SGS_CONV_MASK = 2
 
 # every entry point of include/sgs_b200.h: name -> (restype, argtypes)
 SIGNATURES = {
+    "sgs_quantized_chunks": (ctypes.c_uint32, [ctypes.c_uint32]),
+    "sgs_quantize": (ctypes.c_int, [ctypes.POINTER(Gaussians), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p]),
     "sgs_composite": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p]),

@@ -103,11 +103,14 @@ def render(
     preactivated: torch.Tensor | None = None,
     max_fragments: int = 0,
     max_binned: int = 0,
+    quantized=None,
 ) -> History:
     """One sample-frame (render.py:72-96 of the reference). Keyword-only additions: `preactivated`, the
     `_C.preactivate(scales, rotations, opacities)` tensor of these Gaussians, read by the accumulate
     pass in place of the per-sample covariance and sigmoid (same bits); `max_fragments` and
-    `max_binned`, the GPS point cap and the hybrid queue capacity (0 keeps the reference's values)."""
+    `max_binned`, the GPS point cap and the hybrid queue capacity (0 keeps the reference's values);
+    `quantized`, the `_C.quantize(...)` layout of these Gaussians (16 bytes each, half SH), read in place
+    of the float32 arrays (the images differ by the quantisation)."""
     return History(*_C.render(
         means,
         scales,
@@ -123,4 +126,5 @@ def render(
         preactivated=preactivated,
         max_fragments=max_fragments,
         max_binned=max_binned,
+        quantized=quantized,
     ))

@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
     const uint32_t g = active ? idx : a.n - 1;
 
     Projected p;
-    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre)) return;
+    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre, a.quant)) return;
 
     // importance and number of points (accumulate_scatter.cu:104-112)
     PointSource s;

@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kScatterBlock, kScatterBlocksPerSM) st_scatter
     const uint32_t g = active ? idx : a.n - 1;
 
     Projected p;
-    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre)) return;
+    if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre, a.quant)) return;
     const FrameRng rng = frame_rng(a);
 
     const PixelRect rect = pixel_rect(p.bounds, a.cam);

@@ -24,6 +24,9 @@ int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, Ba
                             "antialiasing");
     if (g->sh_bases != 1 && g->sh_bases != 4 && g->sh_bases != 9 && g->sh_bases != 16)
         return record_error(SGS_ERROR_INVALID_ARGUMENT, "sh_bases must be 1, 4, 9 or 16");
+    if (g->quantized != nullptr)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT,
+                            "the backward pass differentiates the float32 parameters, not the quantised layout");
     if (g->n_gaussians > 0 && (!g->means || !g->scales || !g->rotations || !g->opacities || !g->sh_coefficients))
         return record_error(SGS_ERROR_INVALID_ARGUMENT, "null Gaussian array");
     if (!c->w2c || !c->cam_position) return record_error(SGS_ERROR_INVALID_ARGUMENT, "null camera array");

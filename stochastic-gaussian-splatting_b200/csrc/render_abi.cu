@@ -222,9 +222,17 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     if (s->temporal_mode < SGS_TEMPORAL_RESET || s->temporal_mode > SGS_TEMPORAL_REPROJECT)
         return fail(SGS_ERROR_INVALID_ARGUMENT, "invalid temporal mode %d", s->temporal_mode);
     if (g->n_gaussians > 0) {
-        if (!g->means || !g->scales || !g->rotations || !g->opacities || !g->sh_coefficients)
-            return fail(SGS_ERROR_INVALID_ARGUMENT, "null Gaussian array");
-        if (!aligned16(g->rotations)) return fail(SGS_ERROR_INVALID_ARGUMENT, "rotations must be 16-byte aligned");
+        if (g->quantized != nullptr) {
+            if (!g->quantized_chunks || !g->sh_half || !aligned16(g->quantized) || !aligned16(g->quantized_chunks))
+                return fail(SGS_ERROR_INVALID_ARGUMENT,
+                            "the quantised layout needs 16-byte aligned records and chunk table, and half SH");
+            if (g->preactivated != nullptr)
+                return fail(SGS_ERROR_INVALID_ARGUMENT, "the preactivated and quantised layouts exclude each other");
+        } else {
+            if (!g->means || !g->scales || !g->rotations || !g->opacities || !g->sh_coefficients)
+                return fail(SGS_ERROR_INVALID_ARGUMENT, "null Gaussian array");
+            if (!aligned16(g->rotations)) return fail(SGS_ERROR_INVALID_ARGUMENT, "rotations must be 16-byte aligned");
+        }
         if (!aligned16(g->preactivated))
             return fail(SGS_ERROR_INVALID_ARGUMENT, "the preactivated layout must be 16-byte aligned");
     }
@@ -294,6 +302,9 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     ap.n_samples = n_samples;
     ap.fb_stride = d.n_fb;
     ap.pre = reinterpret_cast<const float4*>(g->preactivated);
+    const QuantizedModel qm{static_cast<const uint4*>(g->quantized), reinterpret_cast<const float4*>(g->quantized_chunks),
+                            static_cast<const __half*>(g->sh_half)};
+    ap.quant = qm;
 
     ResolveParams rp{};
     rp.means = g->means;
@@ -335,6 +346,7 @@ int render_on_streams(const sgs_gaussians* g, const sgs_camera* c, const sgs_set
     rp.temporal_mode = s->temporal_mode;
     rp.n_samples = n_samples;
     rp.fb_stride = d.n_fb;
+    rp.quant = qm;
 
     // the clear and accumulate passes of one framebuffer (or, with p.n_samples > 1, of all of them)
     auto accumulate = [&](const AccumulateParams& p, const size_t n_clear) -> int {

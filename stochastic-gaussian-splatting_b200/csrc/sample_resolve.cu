@@ -37,6 +37,21 @@ constexpr float kBorderMargin = 2.0f;
 
 // View-dependent colour of Gaussian g seen from the camera (resolve.cu:71-76).
 __device__ __forceinline__ float3 winner_color(const ResolveParams& a, const uint32_t g) {
+    if (a.quant.records != nullptr) {
+        // quantised layout: the decoded position and half-precision coefficients
+        const float3 m = quant_position(a.quant, g, a.quant.records[g].x);
+        const float vx = m.x - a.cam_position[0];
+        const float vy = m.y - a.cam_position[1];
+        const float vz = m.z - a.cam_position[2];
+        const float inv_len = rsqrtf(vx * vx + vy * vy + vz * vz);
+        float c[48];
+        const uint32_t nc = a.sh_bases * 3;
+        const __half* src = a.quant.sh + static_cast<size_t>(g) * nc;
+#pragma unroll
+        for (uint32_t i = 0; i < 48; ++i)
+            if (i < nc) c[i] = __half2float(src[i]);
+        return eval_sh(c, vx * inv_len, vy * inv_len, vz * inv_len, a.sh_bases);
+    }
     const float vx = a.means[3 * g + 0] - a.cam_position[0];
     const float vy = a.means[3 * g + 1] - a.cam_position[1];
     const float vz = a.means[3 * g + 2] - a.cam_position[2];
@@ -97,7 +112,7 @@ __global__ void __launch_bounds__(kBlock) reuse_sample_kernel(const ResolveParam
     // the winner projected again, to evaluate it at the neighbours
     bool projected = active && has_sample;
     Projected p;
-    project_gaussian(projected, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p);
+    project_gaussian(projected, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, nullptr, a.quant);
     if (!active) return;
 
     // weights start with the change in alpha; background counts as opaque and farthest

@@ -85,6 +85,7 @@ struct AccumulateParams {
     uint32_t n_samples;               // samples of one call (frames frame .. frame + n_samples - 1)
     size_t fb_stride;                 // framebuffer elements between consecutive samples' framebuffers
     const float4* pre;                // preactivated layout (2 float4 per Gaussian) or null
+    QuantizedModel quant;             // quantised layout (records == null: the float32 arrays)
 };
 
 // Frame-dependent random-number state of one call: the frame index (from device memory when the
@@ -114,6 +115,9 @@ cudaError_t launch_clear(unsigned long long* framebuffer, size_t n_fb, WorkQueue
                          cudaStream_t stream);
 cudaError_t launch_accumulate_st(const AccumulateParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_quantize(const float* means, const float* scales, const float4* rotations, const float* opacities,
+                            const float* sh, uint32_t sh_floats, uint32_t n, uint4* records, float4* chunks,
+                            __half* sh_half, cudaStream_t stream);
 cudaError_t launch_composite(const float* image, const float* depth, const float* alpha, const float* background,
                              uint32_t n, float* rgb, float* depth_out, float* alpha_out, cudaStream_t stream);
 cudaError_t launch_preactivate(const float* scales, const float4* rotations, const float* opacities, uint32_t n,
@@ -155,6 +159,7 @@ struct ResolveParams {
     int temporal_mode;
     uint32_t n_samples;       // samples merged by one call (the first in temporal_mode, the rest Static)
     size_t fb_stride;         // framebuffer elements between consecutive samples' framebuffers
+    QuantizedModel quant;     // quantised layout (records == null: the float32 arrays)
 };
 
 cudaError_t launch_sample_resolve(const ResolveParams& p, cudaStream_t stream);

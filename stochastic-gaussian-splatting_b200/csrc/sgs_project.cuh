@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include "sgs_common.cuh"
 
@@ -41,12 +42,11 @@ struct Cov3d {
     float c11, c12, c13, c22, c23, c33;
 };
 
-__device__ __forceinline__ Cov3d cov3d_of(const uint32_t g, const float* __restrict__ scales,
-                                          const float4* __restrict__ rotations, bool& valid) {
-    const float vx = expf(2.0f * scales[3 * g + 0]);
-    const float vy = expf(2.0f * scales[3 * g + 1]);
-    const float vz = expf(2.0f * scales[3 * g + 2]);
-    const float4 q = rotations[g];
+__device__ __forceinline__ Cov3d cov3d_from(const float s0, const float s1, const float s2, const float4 q,
+                                            bool& valid) {
+    const float vx = expf(2.0f * s0);
+    const float vy = expf(2.0f * s1);
+    const float vz = expf(2.0f * s2);
     const float r = q.x, i = q.y, j = q.z, k = q.w;
     const float ii = i * i, jj = j * j, kk = k * k;
     const float ij = i * j, ik = i * k, jk = j * k;
@@ -70,6 +70,47 @@ __device__ __forceinline__ Cov3d cov3d_of(const uint32_t g, const float* __restr
     return c;
 }
 
+__device__ __forceinline__ Cov3d cov3d_of(const uint32_t g, const float* __restrict__ scales,
+                                          const float4* __restrict__ rotations, bool& valid) {
+    return cov3d_from(scales[3 * g + 0], scales[3 * g + 1], scales[3 * g + 2], rotations[g], valid);
+}
+
+// ---- quantised layout (sgs_quantize, quantize.cu; the README.md:143-147 improvement) ----
+// A Gaussian is one 16-byte record: its position in 11-10-11 bits relative to the box of its chunk
+// of kQuantChunk consecutive Gaussians (the chunk table holds (lo, 0) and (extent, 0) per chunk), its
+// rotation as the three smallest components of the normalised quaternion (2 + 3 x 10 bits), its
+// log-scales and opacity logit as IEEE half; the SH coefficients are IEEE half. records == nullptr
+// selects the float32 arrays.
+constexpr uint32_t kQuantChunk = 256;
+
+struct QuantizedModel {
+    const uint4* records;
+    const float4* chunks;
+    const __half* sh;
+};
+
+__device__ __forceinline__ float quant_half(const uint32_t bits16) {
+    return __half2float(__ushort_as_half(static_cast<unsigned short>(bits16 & 0xffffu)));
+}
+
+__device__ __forceinline__ float3 quant_position(const QuantizedModel& q, const uint32_t g, const uint32_t w) {
+    const float4 lo = q.chunks[2 * (g / kQuantChunk)];
+    const float4 ext = q.chunks[2 * (g / kQuantChunk) + 1];
+    return make_float3(lo.x + static_cast<float>(w >> 21) * (ext.x * (1.0f / 2047.0f)),
+                       lo.y + static_cast<float>((w >> 11) & 1023u) * (ext.y * (1.0f / 1023.0f)),
+                       lo.z + static_cast<float>(w & 2047u) * (ext.z * (1.0f / 2047.0f)));
+}
+
+__device__ __forceinline__ float4 quant_rotation(const uint32_t w) {
+    const uint32_t big = w >> 30;
+    const float c0 = (static_cast<float>((w >> 20) & 1023u) * (2.0f / 1022.0f) - 1.0f) * 0.70710678f;
+    const float c1 = (static_cast<float>((w >> 10) & 1023u) * (2.0f / 1022.0f) - 1.0f) * 0.70710678f;
+    const float c2 = (static_cast<float>(w & 1023u) * (2.0f / 1022.0f) - 1.0f) * 0.70710678f;
+    const float l = sqrtf(fmaxf(0.0f, 1.0f - (c0 * c0 + c1 * c1 + c2 * c2)));
+    return make_float4(big == 0 ? l : c0, big == 1 ? l : (big == 0 ? c0 : c1), big == 2 ? l : (big <= 1 ? c1 : c2),
+                       big == 3 ? l : c2);
+}
+
 // Sigmoid of the opacity logit (gs_utils.h:77-79).
 __device__ __forceinline__ float opacity_of(const float raw_opacity) { return 1.0f / (1.0f + expf(-raw_opacity)); }
 
@@ -90,12 +131,22 @@ __device__ __forceinline__ void preactivated_of(const uint32_t g, const float* _
 // warps from happening.
 // `pre` (nullable): the preactivated layout of the same Gaussians; when given, covariance and
 // opacity are read from it instead of being rebuilt from scales, rotations and the opacity logit.
+// `qm` (records == nullptr: unused): the quantised layout, decoded in place of every float32 array.
 __device__ __forceinline__ bool project_gaussian(bool& active, const uint32_t g, const float* __restrict__ means,
                                                  const float* __restrict__ scales, const float4* __restrict__ rotations,
                                                  const float* __restrict__ opacities, const float4* __restrict__ w2c,
                                                  const PassCamera& cam, Projected& p,
-                                                 const float4* __restrict__ pre = nullptr) {
-    const float mx = means[3 * g + 0], my = means[3 * g + 1], mz = means[3 * g + 2];
+                                                 const float4* __restrict__ pre = nullptr,
+                                                 const QuantizedModel qm = QuantizedModel{}) {
+    uint4 rec = make_uint4(0u, 0u, 0u, 0u);
+    float mx, my, mz;
+    if (qm.records != nullptr) {
+        rec = qm.records[g];
+        const float3 m = quant_position(qm, g, rec.x);
+        mx = m.x, my = m.y, mz = m.z;
+    } else {
+        mx = means[3 * g + 0], my = means[3 * g + 1], mz = means[3 * g + 2];
+    }
     const float4 r3 = w2c[2];
     p.depth = r3.x * mx + r3.y * my + r3.z * mz + r3.w;
     if (p.depth < cam.near_plane || p.depth > cam.far_plane) active = false;
@@ -108,6 +159,10 @@ __device__ __forceinline__ bool project_gaussian(bool& active, const uint32_t g,
         if (p.opacity < kMinAlpha) active = false;
         if (v1.w == 0.0f) active = false;
         cv.c11 = v0.x, cv.c12 = v0.y, cv.c13 = v0.z, cv.c22 = v0.w, cv.c23 = v1.x, cv.c33 = v1.y;
+    } else if (qm.records != nullptr) {
+        p.opacity = opacity_of(quant_half(rec.w >> 16));
+        if (p.opacity < kMinAlpha) active = false;
+        cv = cov3d_from(quant_half(rec.z), quant_half(rec.z >> 16), quant_half(rec.w), quant_rotation(rec.y), active);
     } else {
         p.opacity = opacity_of(opacities[g]);
         if (p.opacity < kMinAlpha) active = false;

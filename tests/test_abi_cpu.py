@@ -138,8 +138,8 @@ def test_python_module_mirrors_the_reference_binding():
                           "history", "view_to_previous_view", "temporal_mode"]
     # additions are keyword-only with defaults, so every reference call binds unchanged
     extras = [p for p in params if p.kind is inspect.Parameter.KEYWORD_ONLY]
-    assert [p.name for p in extras] == ["preactivated", "max_fragments", "max_binned"]
-    assert [p.default for p in extras] == [None, 0, 0]
+    assert [p.name for p in extras] == ["preactivated", "max_fragments", "max_binned", "quantized"]
+    assert [p.default for p in extras] == [None, 0, 0, None]
     assert callable(create_k_buffer)
     with pytest.raises(TypeError):
         _C.render(1, 2, 3)
