@@ -391,6 +391,25 @@ def run_ours(args, world, rank, local) -> dict | None:
                     "preactivate_ms_once": round(p0.elapsed_time(p1), 4), "bytes": pre.numel() * 4}
     del pre
 
+    # opt-in quantised layout (16-byte records and half SH; the images differ by the quantisation)
+    qz = _C.quantize(*scene.tensors())
+    for _ in range(3):
+        hist = _C.render(*scene.tensors(), w2c, pos, *cam_args, *flag_args, blue, *kb, *hist, eye, 1, quantized=qz)
+    torch.cuda.synchronize(dev)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(args.steps):
+        hist = _C.render(*scene.tensors(), w2c, pos, *cam_args, *flag_args, blue, *kb, *hist, eye, 1, quantized=qz)
+    q1.record(stream)
+    torch.cuda.synchronize(dev)
+    q_ms = q0.elapsed_time(q1) / args.steps
+    quantized = {"ms_per_sample": round(q_ms, 5), "sample_frames_per_s": round(1000.0 / q_ms, 2),
+                 "layout_bytes": qz.nbytes(), "float32_bytes": scene_cpu.nbytes(),
+                 "accumulate_algorithmic_bytes_per_launch": 16 * n + qz.chunks.numel() * 4 + 8 * n_fb,
+                 "note": "records of 16 B per Gaussian and half SH; statistical parity with float32 "
+                         "(tests/test_gpu_quantized.py)"}
+    del qz
+
     if rank != 0:
         return None
     peak, peak_kind = hbm_peak()
@@ -440,6 +459,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         "clocks": clock_info,
     }
     line["preactivated"] = preactivated
+    line["quantized"] = quantized
     if not fl["gps"]:
         line["samples_per_call"] = samples_per_call(scene, cam, fl, dev, n_samples=8, calls=max(4, args.steps // 8))
     if not args.no_batch and args.workload.startswith("batch_6m"):
