@@ -82,7 +82,7 @@ struct RowGaussian {
 
 // A published row of the pair stream (64 bytes, four 16-byte words): the packed alpha constants,
 // then depth key and threshold seed, then where its pixels and pairs are.
-struct StreamRow {
+struct __align__(16) StreamRow {
     float mx[2], cx[2];      // shifted mean x and exp2-scaled conic x, each twice (packed FP32x2 operands)
     float cydy[2], czdy[2];  // cy * dy and cz * dy, each twice
     float dy, opacity;
@@ -390,15 +390,18 @@ __global__ void __launch_bounds__(kScatterBlock, kScatterBlocksPerSM) st_scatter
         }
     }
 
-    // level 1: the rows of this warp's Gaussians, end to end in lane order, 32 rows at a time
+    // level 1: the rows of this warp's Gaussians, end to end in lane order, 32 rows at a time. A row's
+    // owner is found as the ordinal of its Gaussian among the warp's Gaussians with rows (the count of
+    // row starts up to it), so each Gaussian's constants are stored at that ordinal
     const uint32_t h = has_rows ? rect.height : 0u;
     const uint32_t incl_rows = warp_inclusive_sum(h, lane);
     const uint32_t total_rows = __shfl_sync(kFullMask, incl_rows, 31);
     const uint32_t row_first = incl_rows - h;
+    const uint32_t with_rows = __ballot_sync(kFullMask, has_rows);
     if (has_rows) {
         RowGaussian st = G;
         st.row_first = row_first;
-        s_gauss[wib][lane] = st;
+        s_gauss[wib][__popc(with_rows & lt_mask)] = st;
     }
     StreamRow* ring = s_ring[wib];
     uint32_t* bitmap = s_bits[wib];

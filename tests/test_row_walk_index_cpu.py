@@ -205,3 +205,43 @@ def test_pair_stream_capacity_bounds():
     _, _, _, live, words = run_pair_stream(batches)
     assert live <= STREAM_ROWS and words <= STREAM_WORDS
     assert live == 63
+
+
+def level1_owner_slots(heights: list[int]) -> list[tuple[int, int]]:
+    """st_scatter_kernel's level 1 for one warp: lane l's Gaussian has heights[l] AABB rows (0: culled,
+    queued or empty). Rows are laid end to end in lane order; each Gaussian with rows is stored at slot
+    popc(lanes with rows below it); a row finds its slot as `prev + popc(row starts up to it)` over
+    32-row batches. Returns, per row, (slot read, lane the slot was written by)."""
+    with_rows = [h > 0 for h in heights]
+    incl, row_first, slots = 0, [], {}
+    for lane, h in enumerate(heights):
+        row_first.append(incl)
+        incl += h
+        if with_rows[lane]:
+            slots[sum(with_rows[:lane])] = lane
+    total = incl
+    out, prev = [], -1
+    for base in range(0, total, 32):
+        bits = 0
+        for lane in range(32):
+            rel = row_first[lane] - base
+            if with_rows[lane] and 0 <= rel < 32:
+                bits |= 1 << rel
+        for lane in range(32):
+            r = base + lane
+            owner = prev + bin(bits & ((1 << (lane + 1)) - 1)).count("1")
+            if r < total:
+                out.append((owner, slots[owner]))
+        prev += bin(bits).count("1")
+    return out
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_level1_rows_find_their_own_gaussian(seed):
+    """Every row reads the constants of the Gaussian it belongs to, also with Gaussians without rows
+    between them (a lane-indexed store would hand those rows another Gaussian's or an unwritten slot)."""
+    rng = random.Random(seed)
+    heights = [0 if rng.random() < 0.4 else rng.randint(1, rng.choice([3, 40, 200])) for _ in range(32)]
+    want = [lane for lane, h in enumerate(heights) for _ in range(h)]
+    got = [lane for _, lane in level1_owner_slots(heights)]
+    assert got == want
