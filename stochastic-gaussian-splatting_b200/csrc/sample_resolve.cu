@@ -35,23 +35,26 @@ constexpr float kMinExtentLuma = 0.01f;
 constexpr float kMinExtentChroma = 0.005f;
 constexpr float kBorderMargin = 2.0f;
 
+// Colour of Gaussian g in the quantised layout: its decoded position and half-precision SH. A
+// separate, non-inlined function, so that the float32 path's code (whose rounding the reference's
+// bits depend on) is compiled exactly as without it.
+__device__ __noinline__ float3 quantized_color(const QuantizedModel q, const float* __restrict__ cam_position,
+                                              const uint32_t sh_bases, const uint32_t g) {
+    const float3 m = quant_position(q, g, q.records[g].x);
+    const float vx = m.x - cam_position[0];
+    const float vy = m.y - cam_position[1];
+    const float vz = m.z - cam_position[2];
+    const float inv_len = rsqrtf(vx * vx + vy * vy + vz * vz);
+    float c[48];
+    const uint32_t nc = sh_bases * 3;
+    const __half* src = q.sh + static_cast<size_t>(g) * nc;
+    for (uint32_t i = 0; i < nc; ++i) c[i] = __half2float(src[i]);
+    return eval_sh(c, vx * inv_len, vy * inv_len, vz * inv_len, sh_bases);
+}
+
 // View-dependent colour of Gaussian g seen from the camera (resolve.cu:71-76).
 __device__ __forceinline__ float3 winner_color(const ResolveParams& a, const uint32_t g) {
-    if (a.quant.records != nullptr) {
-        // quantised layout: the decoded position and half-precision coefficients
-        const float3 m = quant_position(a.quant, g, a.quant.records[g].x);
-        const float vx = m.x - a.cam_position[0];
-        const float vy = m.y - a.cam_position[1];
-        const float vz = m.z - a.cam_position[2];
-        const float inv_len = rsqrtf(vx * vx + vy * vy + vz * vz);
-        float c[48];
-        const uint32_t nc = a.sh_bases * 3;
-        const __half* src = a.quant.sh + static_cast<size_t>(g) * nc;
-#pragma unroll
-        for (uint32_t i = 0; i < 48; ++i)
-            if (i < nc) c[i] = __half2float(src[i]);
-        return eval_sh(c, vx * inv_len, vy * inv_len, vz * inv_len, a.sh_bases);
-    }
+    if (a.quant.records != nullptr) return quantized_color(a.quant, a.cam_position, a.sh_bases, g);
     const float vx = a.means[3 * g + 0] - a.cam_position[0];
     const float vy = a.means[3 * g + 1] - a.cam_position[1];
     const float vz = a.means[3 * g + 2] - a.cam_position[2];
