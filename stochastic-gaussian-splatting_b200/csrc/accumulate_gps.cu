@@ -176,14 +176,22 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
                 base = __shfl_sync(kFullMask, base, leader);
                 const uint32_t e = static_cast<uint32_t>(base >> kQueueEntryShift) + __popc(ballot & ((1u << lane) - 1u));
                 const unsigned long long first_chunk = (base & kQueueChunkMask) + (incl - chunks);
-                if (want && e < a.max_binned && e < a.q.capacity && first_chunk + chunks <= kMaxQueueChunks) {
-                    a.q.key[e] = s.key;
-                    a.q.geom[e] = make_float4(s.mean2d.x, s.mean2d.y, s.L.x, s.L.y);
-                    a.q.geom2[e] = make_float4(s.L.z, s.power_threshold, s.opacity_rcp, s.opacity_dilog);
-                    a.q.meta[e] = make_uint4(__float_as_uint(s.conic.x), __float_as_uint(s.conic.y),
-                                             __float_as_uint(s.conic.z), static_cast<uint32_t>(first_chunk));
-                    a.q.count[e] = count;
-                    act = false;
+                if (want && e < a.max_binned && e < a.q.capacity) {
+                    if (first_chunk + chunks <= kMaxQueueChunks) {
+                        a.q.key[e] = s.key;
+                        a.q.geom[e] = make_float4(s.mean2d.x, s.mean2d.y, s.L.x, s.L.y);
+                        a.q.geom2[e] = make_float4(s.L.z, s.power_threshold, s.opacity_rcp, s.opacity_dilog);
+                        a.q.meta[e] = make_uint4(__float_as_uint(s.conic.x), __float_as_uint(s.conic.y),
+                                                 __float_as_uint(s.conic.z), static_cast<uint32_t>(first_chunk));
+                        a.q.count[e] = count;
+                        act = false;
+                    } else {
+                        // past 32-bit chunk indices (where the reference's own chunk offsets wrap): the
+                        // entry is marked unused and the Gaussian scattered. Entries and chunks are
+                        // reserved together, so the marked entries are the queue's last ones.
+                        a.q.meta[e] = make_uint4(0u, 0u, 0u, kUnusedQueueEntry);
+                        a.q.count[e] = 0u;
+                    }
                 }
             }
         }
@@ -256,8 +264,11 @@ __global__ void __launch_bounds__(kBlock, kQueueBlocksPerSM) gps_queue_kernel(co
     const uint32_t cap = min(a.max_binned, a.q.capacity);
     const uint32_t n_entries = static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(cap)));
     if (n_entries == 0) return;
-    const uint32_t last_first = a.q.meta[n_entries - 1].w;
-    const uint32_t n_chunks = last_first + (a.q.count[n_entries - 1] + kChunkPoints - 1) / kChunkPoints;
+    // the last used entry (entry 0, which starts at chunk 0, always is); marked entries start past
+    // every chunk, so the search below never lands on one
+    uint32_t last = n_entries - 1;
+    if (a.q.meta[last].w == kUnusedQueueEntry) last = queue_entry_of_chunk(a.q.meta, n_entries, kUnusedQueueEntry - 1u, lane);
+    const uint32_t n_chunks = a.q.meta[last].w + (a.q.count[last] + kChunkPoints - 1) / kChunkPoints;
     const uint32_t frame = frame_rng(a).frame;
     for (;;) {
         uint32_t c0 = 0;

@@ -387,6 +387,9 @@ __global__ void __launch_bounds__(kScatterBlock, kScatterBlocksPerSM) st_scatter
         } else {
             keep_big = true;
             atomicAdd(&a.queue->overflow, 1u);
+            // an entry past 32-bit chunk indices is marked unused (the marked entries are the last ones:
+            // entries and chunks are reserved together)
+            if (e < a.q.capacity) a.q.meta[e] = make_uint4(0u, 0u, 0u, kUnusedQueueEntry);
         }
     }
 
@@ -502,7 +505,10 @@ __global__ void __launch_bounds__(kBlock) st_queue_kernel(const AccumulateParams
     const uint32_t n_entries =
         static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(a.q.capacity)));
     if (n_entries == 0) return;
-    const uint4 last = a.q.meta[n_entries - 1];
+    uint32_t last_entry = n_entries - 1;  // the last used entry; entry 0 starts at chunk 0 and always is
+    if (a.q.meta[last_entry].w == kUnusedQueueEntry)
+        last_entry = queue_entry_of_chunk(a.q.meta, n_entries, kUnusedQueueEntry - 1u, lane);
+    const uint4 last = a.q.meta[last_entry];
     const uint32_t last_log_rpc = last.z & ~kGatherFormFlag;
     const uint32_t n_chunks = last.w + ((last.y + (1u << last_log_rpc) - 1u) >> last_log_rpc);
     for (;;) {

@@ -364,11 +364,14 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
             const unsigned long long old = atomicAdd(&b.bw_queue->packed, (1ull << kQueueEntryShift) | chunks);
             const uint32_t e = static_cast<uint32_t>(old >> kQueueEntryShift);
             const unsigned long long first_chunk = old & kQueueChunkMask;
-            if (e < b.bw_capacity && first_chunk + chunks <= 0xffffffffull) {
+            if (e < b.bw_capacity && first_chunk + chunks <= kMaxQueueChunks) {
                 static_cast<WalkGaussian*>(b.bw_entries)[e] = q;
                 b.bw_meta[e] = make_uint4(rect.y_min, rect.height, log_rpc, static_cast<uint32_t>(first_chunk));
                 b.bw_index[e] = g;
                 has_rows = false;
+            } else if (e < b.bw_capacity) {
+                // past 32-bit chunk indices: marked unused (the marked entries are the last ones), walked here
+                b.bw_meta[e] = make_uint4(0u, 0u, 0u, kUnusedQueueEntry);
             }
         }
     }
@@ -420,7 +423,10 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const B
     const uint32_t n_entries =
         static_cast<uint32_t>(min(packed >> kQueueEntryShift, static_cast<unsigned long long>(b.bw_capacity)));
     if (n_entries == 0) return;
-    const uint4 last = b.bw_meta[n_entries - 1];
+    uint32_t last_entry = n_entries - 1;  // the last used entry; entry 0 starts at chunk 0 and always is
+    if (b.bw_meta[last_entry].w == kUnusedQueueEntry)
+        last_entry = queue_entry_of_chunk(b.bw_meta, n_entries, kUnusedQueueEntry - 1u, lane);
+    const uint4 last = b.bw_meta[last_entry];
     const uint32_t n_chunks = last.w + ((last.y + (1u << last.z) - 1u) >> last.z);
     const WalkGaussian* entries = static_cast<const WalkGaussian*>(b.bw_entries);
     for (;;) {

@@ -77,11 +77,9 @@ int derive(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, D
             if (s->hybrid_scheduling) {
                 d.max_binned = s->max_binned != 0 ? s->max_binned : std::min(g->n_gaussians, kDefaultMaxBinned);
                 d.max_binned = std::min(d.max_binned, g->n_gaussians);
-                // every entry's chunk range must fit 32-bit chunk indices
-                const uint64_t cap_points = s->max_fragments != 0 ? s->max_fragments : (fbw * fbh) / 2 + 1;
-                const uint64_t max_chunks = (cap_points + 255) / 256;
-                const uint64_t limit = 0xffffffffull / std::max<uint64_t>(max_chunks, 1);
-                if (d.max_binned > limit) d.max_binned = static_cast<uint32_t>(limit);
+                // an entry whose chunks would pass 32-bit chunk indices is not binned (the producer
+                // marks it and scatters its Gaussian), so the queue holds max_binned entries like the
+                // reference's bin
                 d.queue_capacity = d.max_binned;
             }
         } else {

@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kBlock) plain_sample_kernel(const ResolveParam
 // Advances a device-resident frame index once per call. The last pass of a call does it: every
 // pass that reads the index (accumulate) has finished by then in stream order.
 __device__ __forceinline__ void advance_frame(const ResolveParams& a) {
-    if (a.frame_counter != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *a.frame_counter += 1u;
+    if (a.frame_counter != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *a.frame_counter += 1u;
 }
 
 __device__ __forceinline__ float3 rgb_to_ycocg(const float3 c) {
@@ -481,22 +481,30 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
 #pragma unroll
                 for (uint32_t i = 0; i < 4; ++i) {
                     const float w = wx[i] * wy[j];
+                    // the texel from shared memory or from the history arrays, then one accumulation for
+                    // both (the same operations either way)
+                    float hr, hg, hb, hd, ha;
                     if (staged_history) {
                         const uint32_t k = (hy + j - by0) * bw + (hx + i - bx0);
                         const uint32_t cap = L.hist_cap;
-                        ch.x += w * s_hist[k];
-                        ch.y += w * s_hist[cap + k];
-                        ch.z += w * s_hist[2 * cap + k];
-                        dh += w * s_hist[3 * cap + k];
-                        ah += w * s_hist[4 * cap + k];
+                        hr = s_hist[k];
+                        hg = s_hist[cap + k];
+                        hb = s_hist[2 * cap + k];
+                        hd = s_hist[3 * cap + k];
+                        ha = s_hist[4 * cap + k];
                     } else {
                         const uint32_t hi = (hy + j) * a.width + hx + i;
-                        ch.x += w * a.hist_image[3 * hi + 0];
-                        ch.y += w * a.hist_image[3 * hi + 1];
-                        ch.z += w * a.hist_image[3 * hi + 2];
-                        dh += w * a.hist_depth[hi];
-                        ah += w * a.hist_alpha[hi];
+                        hr = a.hist_image[3 * hi + 0];
+                        hg = a.hist_image[3 * hi + 1];
+                        hb = a.hist_image[3 * hi + 2];
+                        hd = a.hist_depth[hi];
+                        ha = a.hist_alpha[hi];
                     }
+                    ch.x += w * hr;
+                    ch.y += w * hg;
+                    ch.z += w * hb;
+                    dh += w * hd;
+                    ah += w * ha;
                 }
             }
 

@@ -24,6 +24,9 @@ constexpr unsigned long long kQueueChunkMask = (1ull << kQueueEntryShift) - 1;
 // Producers queue chunk indices below this, so the consumers' cursor (which overshoots the last chunk
 // by at most one claim per warp) cannot wrap around.
 constexpr unsigned long long kMaxQueueChunks = 0xffffffffull - (1ull << 24);
+// First-chunk value of a queue entry left unused because its chunks would pass
+// kMaxQueueChunks (above every chunk index, so the entry search never returns it).
+constexpr uint32_t kUnusedQueueEntry = 0xffffffffu;
 
 // Per-entry arrays of the large-Gaussian queue (structure of arrays, 16-byte aligned).
 struct QueueArrays {

@@ -76,6 +76,24 @@ def test_workspace_size_and_layout():
     assert size2 >= 4 * 40 * n_fb  # fb + samples + reuse weights at 4x the subpixels
 
 
+def test_hybrid_gps_queue_holds_the_reference_bin():
+    """The hybrid-GPS queue holds min(N, 2^20) entries whatever the framebuffer size, like the
+    reference's bin (accumulate_hybrid_gps.cu:22,202): at 1280x720 with supersampling 2 a 1M-Gaussian
+    scene bins up to 1M Gaussians. An entry whose chunks would pass 32-bit chunk indices is marked
+    unused on the device instead of the queue being shortened."""
+    lib = _abi.load()
+
+    def size(n, max_binned=0):
+        g, c, s = _args(n=n, width=1280, height=720, ss=2, gps=1, hybrid=1)
+        s.max_binned = max_binned
+        return lib.sgs_workspace_size(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s))
+
+    entry_bytes = 8 + 16 + 16 + 16 + 4  # key, two geometry float4s, meta, point count
+    grown = size(1_000_000) - size(1_000_000, max_binned=500_000)
+    assert abs(grown - 500_000 * entry_bytes) <= 5 * 256
+    assert size(2_000_000) == size(2_000_000, max_binned=1 << 20)
+
+
 def test_invalid_arguments_are_rejected_before_any_launch():
     lib = _abi.load()
     h = _abi.HistoryC()

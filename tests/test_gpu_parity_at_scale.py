@@ -12,7 +12,7 @@ N(-4.5, 0.8^2), opacity logits N(0, 2^2), degree-3 SH; seed 0) seen from the orb
 * the GPS-hybrid progressive workload at full size (1M heavy-tailed Gaussians, 1280x720,
   supersampling 2, orbit radius 4, spatial reuse, Reproject between views, Static within a view)
   through the reference's own `_C.render`, and the same workload with its caps (max_fragments 1024,
-  max_binned 65536) against the reference built with those two constants changed.
+  max_binned 65536) against the reference built with those two constants changed (80k Gaussians).
 """
 import numpy as np
 import pytest
@@ -180,12 +180,12 @@ def test_gps_hybrid_progressive_full_size_bitwise(ref, cuda_device):
 
 def test_gps_hybrid_progressive_workload_caps_bitwise(cuda_device):
     """The workload's caps (max_fragments 1024, max_binned 65536) against the reference built with those
-    two constants (oracle/build_ref.py), on 100k Gaussians of the workload's distribution, where every
+    two constants (oracle/build_ref.py), on 80k Gaussians of the workload's distribution, where every
     qualifying Gaussian fits the 65,536-entry bin: beyond it the reference itself picks the binned
     Gaussians by atomic arrival order, and its images are not reproducible bit for bit."""
     ref_c1 = build_ref.load_c1()
     caps = dict(max_fragments=build_ref.C1_MAX_FRAGMENTS, max_binned=build_ref.C1_MAX_BINNED)
-    spec = sgs_scenes.SceneSpec(n=100_000, log_scale_mean=-3.0, log_scale_std=1.0)
+    spec = sgs_scenes.SceneSpec(n=80_000, log_scale_mean=-3.0, log_scale_std=1.0)
     scene = sgs_scenes.make_scene(spec, seed=3).to(cuda_device)
     cams = sgs_scenes.orbit_cameras(16, 4.0, C1_W, C1_H)[:4]
     for cam in cams:
