@@ -10,9 +10,9 @@
 // in the cooperative phase, for every point it evaluates of the warp's larger Gaussians, in lane
 // order. The winners therefore depend on that exact warp grouping and draw order, and this
 // kernel keeps both (culled and padding lanes still draw their Poisson sample). It evaluates the
-// points in another order where that pays: the lanes' own first points and the last partial row of
-// each cooperative Gaussian are drawn in stream order, parked as stream states in a per-warp
-// buffer and evaluated 32 at a time whatever lane or Gaussian they belong to.
+// points in another order where that pays: the last partial row of each cooperative Gaussian is
+// drawn in stream order, parked as stream states in a per-warp buffer and evaluated 32 at a time
+// whatever Gaussian it belongs to.
 //
 // Hybrid scheduling bins the Gaussians with more than 512 points (up to max_binned of them) into
 // the device-side work queue; their points use counter-based seeds (seed ^ point * golden
@@ -30,8 +30,7 @@ constexpr uint32_t kFullMask = 0xffffffffu;
 constexpr uint32_t kBinningPointThreshold = 512;  // accumulate_hybrid_gps.cu:21
 constexpr uint32_t kChunkPoints = 256;             // accumulate_hybrid_gps.cu:19
 constexpr uint32_t kQueueBlocksPerSM = 8;
-constexpr uint32_t kItemsPerWarp = 128;  // parked points per warp (multiple of 32)
-static_assert(kItemsPerWarp >= 32 * kSequentialFragments, "every lane's own first points fit the buffer");
+constexpr uint32_t kItemsPerWarp = 128;  // parked cooperative points per warp (multiple of 32)
 constexpr uint32_t kChunksPerClaim = 8;  // chunks a consumer warp takes per atomic on the cursor
 
 struct PointSource {
@@ -196,30 +195,8 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
             }
         }
 
-        // Own first points (scatter_utils.cuh:34-47): each lane draws its first min(count, 4) points from
-        // its own stream, in order; they are parked in the warp's buffer (32 lanes x 4 = its 128 items)
-        // and evaluated 32 at a time across the lanes, instead of each lane evaluating its own points
-        // while the lanes with fewer points wait (about 40 % of the lane-steps did work on the
-        // 6M-Gaussian 1080p scene).
-        {
-            const uint32_t own = act ? min(count, kSequentialFragments) : 0u;
-            uint32_t incl = own;
-#pragma unroll
-            for (uint32_t o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(kFullMask, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const uint32_t n_own = __shfl_sync(kFullMask, incl, 31);
-            if (n_own != 0) {
-                __syncwarp();
-                for (uint32_t i = 0, at = incl - own; i < own; ++i, ++at) {
-                    pcg2d_step(seed);
-                    s_state[warp][at] = seed;
-                    s_src[warp][at] = static_cast<uint8_t>(lane);
-                }
-                evaluate_parked(a, fb, s, s_state[warp], s_src[warp], n_own, lane);
-            }
-        }
+        // own first points, sequentially per lane (scatter_utils.cuh:34-47)
+        for (uint32_t i = 0; act && i < count && i < kSequentialFragments; ++i) gps_point(a, fb, seed, s);
 
         // The rest cooperatively, the warp's larger Gaussians in lane order: point j (after the first
         // kSequentialFragments) of Gaussian src is drawn by lane j % 32 from its own stream, in (src, j)

@@ -7,19 +7,14 @@
 // pixel) and the merge is a minimum, so the result does not depend on which thread evaluates
 // which fragment. This file uses that freedom for a B200-oriented schedule:
 //
-//  * rows, then spans: a warp expands its 32 Gaussians into AABB rows, 32 rows at a time, and
-//    each lane computes the conservative x-span of the alpha >= 1/255 ellipse on its row (the AABB
-//    corners, ~45% of its pixels, are never evaluated);
-//  * a pixel-pair stream per warp: every non-empty span is published to a small shared-memory ring
-//    (the row's alpha and threshold constants, its first pair in the warp's stream) and its first
-//    pair sets one bit of a row-start bitmap; the warp then consumes the stream 32 pairs at a time,
-//    one pair of adjacent pixels per lane, the owning row found with one popc of that bitmap word.
-//    Rows of 1 to 128 pixels (almost all of them) so keep every lane busy, where walking one row
-//    per lane made a warp step as often as its longest row needed (under half of the lane-steps
-//    did work on the 6M-Gaussian 1080p scene). Both pixels' alpha exponents are evaluated with
+//  * rows, then spans: a warp sorts its 32 Gaussians by their widest span (a bitonic network over
+//    the lanes), expands them into AABB rows in that order, 32 rows at a time, and each lane
+//    computes the conservative x-span of the alpha >= 1/255 ellipse on its row (the AABB corners,
+//    ~45% of its pixels, are never evaluated);
+//  * each lane then walks its own row two pixels per step, the alpha exponent of both pixels in
 //    packed FP32x2 instructions (fma/mul/sub .f32x2 of sm_100a, each element rounded like the scalar
-//    instruction); each accepted pixel issues one predicated RED. Longer rows are walked one row per
-//    lane;
+//    instruction), with no per-pixel owner lookup or shared-memory traffic; the warp steps as often
+//    as its longest row needs, and each accepted pixel issues one predicated RED;
 //  * a device-side work queue for Gaussians covering more than kBigFragments pixels: their rows are
 //    cut into chunks of about kChunkPixels pixels that a persistent kernel steals across all SMs (no
 //    cross-warp tail, no host synchronisation). A chunk has R rows (a power of two <= 32) and each
@@ -43,18 +38,8 @@
 namespace sgs {
 namespace {
 
-constexpr uint32_t kBlock = 256;              // queue kernel
-constexpr uint32_t kScatterBlock = 128;       // scatter kernel: 4 warps, each with its own pair stream
-constexpr uint32_t kScatterWarps = kScatterBlock / 32;
-constexpr uint32_t kScatterBlocksPerSM = 8;
-// Pair stream of a scatter warp: ring of published rows and ring of row-start bitmap words (powers of
-// two). At most 31 rows hold pairs left over from a window when a batch of 32 rows is published, so
-// 64 ring entries hold every live row; a batch adds at most 32 x kStreamMaxPairs pairs, so 128
-// bitmap words (4096 pairs) cover every pair not yet consumed.
-constexpr uint32_t kStreamRows = 64;
-constexpr uint32_t kStreamWords = 128;
-// Rows with more pixels than 2 x kStreamMaxPairs are walked one row per lane instead.
-constexpr uint32_t kStreamMaxPairs = 64;
+constexpr uint32_t kBlock = 256;
+constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kFullMask = 0xffffffffu;
 // Gaussians whose AABB exceeds this many pixels go to the work queue.
 constexpr uint32_t kBigFragments = 2048;
@@ -79,20 +64,6 @@ struct RowGaussian {
     uint32_t row_first; // first row position in the warp's row list (level 1)
     uint32_t flags;     // kGatherFormFlag
 };
-
-// A published row of the pair stream (64 bytes, four 16-byte words): the packed alpha constants,
-// then depth key and threshold seed, then where its pixels and pairs are.
-struct __align__(16) StreamRow {
-    float mx[2], cx[2];      // shifted mean x and exp2-scaled conic x, each twice (packed FP32x2 operands)
-    float cydy[2], czdy[2];  // cy * dy and cz * dy, each twice
-    float dy, opacity;
-    uint32_t key_lo, key_hi;
-    uint32_t seed;           // white noise: the row seed; blue noise: slice row texel | x offset << 16
-    uint32_t x0;             // first pixel's x | kGatherFormFlag
-    uint32_t start_len;      // first pair in the warp's stream | pixels << 24
-    uint32_t index;          // framebuffer index of the first pixel
-};
-static_assert(sizeof(StreamRow) == 64, "four 16-byte words");
 
 // Packed FP32x2 arithmetic (sm_100a): two independent round-to-nearest operations per instruction,
 // bit-identical to the scalar __fsub_rn / __fmul_rn / __fmaf_rn of each element.
@@ -160,6 +131,23 @@ __device__ __forceinline__ uint32_t row_seed(const FrameRng& rng, const uint32_t
     return key_lo ^ (rng.frame * 1973u) ^ (y * 2699u);
 }
 
+// Sorting key of Gaussians without rows (they go after every Gaussian with rows).
+constexpr uint32_t kNoRowsKey = (1u << 26) - 1u;
+
+// Bitonic sort of one 32-bit value per lane, ascending over the lanes (values distinct).
+__device__ __forceinline__ uint32_t warp_sort_ascending(uint32_t v, const uint32_t lane) {
+#pragma unroll
+    for (uint32_t k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t other = __shfl_xor_sync(kFullMask, v, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = keep_min ? min(v, other) : max(v, other);
+        }
+    }
+    return v;
+}
+
 // One predicated 64-bit RED.MIN (no branch around it).
 __device__ __forceinline__ void red_min_if(unsigned long long* address, const unsigned long long key, const bool pred) {
     asm volatile(
@@ -168,64 +156,9 @@ __device__ __forceinline__ void red_min_if(unsigned long long* address, const un
         : "memory");
 }
 
-// Alpha tests and thresholds of pixels x0 and x0 + 1 of one row (scatter_utils.cuh:35-46 per pixel):
-// `px` points at pixel x0 of the framebuffer (of the first sample), fx holds (x0, x0 + 1) as floats,
-// the other operands are the row's constants, each held twice for the packed FP32x2 instructions.
-// in0 / in1: the pixel lies in the row's span. Every lane of the warp calls it (the callers keep the
-// warp converged).
-template <bool kBlue, bool kHybrid, bool kMulti>
-__device__ __forceinline__ void eval_pair(const AccumulateParams& a, const FrameRng& rng, unsigned long long* px,
-                                          const uint32_t x0, const unsigned long long fx,
-                                          const unsigned long long mx2, const unsigned long long cx2,
-                                          const unsigned long long cydy2, const unsigned long long czdy2,
-                                          const unsigned long long dy2, const unsigned long long opacity2,
-                                          const unsigned long long key, const uint32_t seed, const uint32_t bx,
-                                          const bool gather_form, const bool in0, const bool in1) {
-    // alpha of both pixels with the reference's contraction of the exponent
-    const unsigned long long dx = f2_sub(fx, mx2);
-    const unsigned long long inner = f2_fma(cx2, dx, cydy2);
-    const unsigned long long e2 =
-        kHybrid && gather_form ? f2_fma(dx, inner, f2_mul(czdy2, dy2)) : f2_fma(czdy2, dy2, f2_mul(dx, inner));
-    const float2 e = f2_unpack(e2);
-    const float2 alpha = f2_unpack(f2_mul(opacity2, f2_pack(exp2f(fminf(e.x, 0.0f)), exp2f(fminf(e.y, 0.0f)))));
-    if (!kMulti) {
-        float2 u;
-        if (kBlue) {
-            u = make_float2(st_blue_threshold(rng, seed, x0, bx), st_blue_threshold(rng, seed, x0 + 1u, bx));
-        } else {
-            u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed, x0)),
-                                         __uint_as_float(st_threshold_bits(seed, x0 + 1u))),
-                                 f2_pack(1.0f, 1.0f)));
-        }
-        red_min_if(px, key, in0 && alpha.x >= kMinAlpha && u.x < alpha.x);
-        red_min_if(px + 1, key, in1 && alpha.y >= kMinAlpha && u.y < alpha.y);
-    } else {
-        // the same two pixels in every sample of the call: alpha once, one threshold per frame
-        const bool ok0 = in0 && alpha.x >= kMinAlpha;
-        const bool ok1 = in1 && alpha.y >= kMinAlpha;
-        unsigned long long* px_s = px;
-        for (uint32_t sm = 0; sm < a.n_samples; ++sm, px_s += a.fb_stride) {
-            const uint32_t frame = rng.frame + sm;
-            float2 u;
-            if (kBlue) {
-                const FrameRng rs = frame_rng_at(a, frame);
-                u = make_float2(st_blue_threshold(rs, seed, x0, bx), st_blue_threshold(rs, seed, x0 + 1u, bx));
-            } else {
-                // row seeds differ between frames only in the frame term
-                const uint32_t seed_s = seed ^ ((rng.frame * 1973u) ^ (frame * 1973u));
-                u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed_s, x0)),
-                                             __uint_as_float(st_threshold_bits(seed_s, x0 + 1u))),
-                                     f2_pack(1.0f, 1.0f)));
-            }
-            red_min_if(px_s, key, ok0 && u.x < alpha.x);
-            red_min_if(px_s + 1, key, ok1 && u.y < alpha.y);
-        }
-    }
-}
-
 // Each lane walks segment `seg` of `1 << log_segs` equal parts of the span of its row y (when
-// valid), two pixels per step; the warp takes as many steps as its longest segment needs. Used for
-// queued Gaussians' chunks, rows longer than the pair stream takes, and the queue's overflow.
+// valid), two pixels per step; the warp takes as many steps as its longest segment needs
+// (scatter_utils.cuh:35-46 per pixel).
 template <bool kBlue, bool kHybrid, bool kMulti>
 __device__ __forceinline__ void walk_rows(const AccumulateParams& a, const FrameRng& rng, const bool valid,
                                           const RowGaussian& G, const uint32_t y, const uint32_t seg = 0,
@@ -258,46 +191,50 @@ __device__ __forceinline__ void walk_rows(const AccumulateParams& a, const Frame
     const float fxs = static_cast<float>(xs);  // pixel coordinates are exact in float
     unsigned long long fx = f2_pack(fxs, fxs + 1.0f);
     for (uint32_t i = 0; i < steps; i += 2) {
-        eval_pair<kBlue, kHybrid, kMulti>(a, rng, row + i, xs + i, fx, mx2, cx2, cydy2, czdy2, dy2, opacity2, key,
-                                          seed, bx, gather_form, i < len, i + 1u < len);
+        // alpha of pixels xs + i and xs + i + 1 with the reference's contraction of the exponent
+        const unsigned long long dx = f2_sub(fx, mx2);
+        const unsigned long long inner = f2_fma(cx2, dx, cydy2);
+        const unsigned long long e2 =
+            gather_form ? f2_fma(dx, inner, f2_mul(czdy2, dy2)) : f2_fma(czdy2, dy2, f2_mul(dx, inner));
+        const float2 e = f2_unpack(e2);
+        const float2 alpha =
+            f2_unpack(f2_mul(opacity2, f2_pack(exp2f(fminf(e.x, 0.0f)), exp2f(fminf(e.y, 0.0f)))));
+        const uint32_t x0 = xs + i;
+        if (!kMulti) {
+            float2 u;
+            if (kBlue) {
+                u = make_float2(st_blue_threshold(rng, seed, x0, bx), st_blue_threshold(rng, seed, x0 + 1u, bx));
+            } else {
+                u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed, x0)),
+                                             __uint_as_float(st_threshold_bits(seed, x0 + 1u))),
+                                     f2_pack(1.0f, 1.0f)));
+            }
+            red_min_if(row + i, key, i < len && alpha.x >= kMinAlpha && u.x < alpha.x);
+            red_min_if(row + i + 1u, key, i + 1u < len && alpha.y >= kMinAlpha && u.y < alpha.y);
+        } else {
+            // the same two pixels in every sample of the call: alpha once, one threshold per frame
+            const bool in_x = i < len && alpha.x >= kMinAlpha;
+            const bool in_y = i + 1u < len && alpha.y >= kMinAlpha;
+            unsigned long long* row_s = row;
+            for (uint32_t sm = 0; sm < a.n_samples; ++sm, row_s += a.fb_stride) {
+                const uint32_t frame = rng.frame + sm;
+                float2 u;
+                if (kBlue) {
+                    const FrameRng rs = frame_rng_at(a, frame);
+                    u = make_float2(st_blue_threshold(rs, seed, x0, bx), st_blue_threshold(rs, seed, x0 + 1u, bx));
+                } else {
+                    // row seeds differ between frames only in the frame term
+                    const uint32_t seed_s = seed ^ ((rng.frame * 1973u) ^ (frame * 1973u));
+                    u = f2_unpack(f2_sub(f2_pack(__uint_as_float(st_threshold_bits(seed_s, x0)),
+                                                 __uint_as_float(st_threshold_bits(seed_s, x0 + 1u))),
+                                         f2_pack(1.0f, 1.0f)));
+                }
+                red_min_if(row_s + i, key, in_x && u.x < alpha.x);
+                red_min_if(row_s + i + 1u, key, in_y && u.y < alpha.y);
+            }
+        }
         fx = f2_add(fx, two);
     }
-}
-
-// One window of the pair stream: pairs [window, window + 32) of the warp's published rows, pair
-// window + lane on this lane. `bits` marks the rows that start in the window (bit i: a row's first
-// pair is window + i) and `rows_before` counts the rows that start before it, so the lane's row is
-// row rows_before + popc(bits up to the lane) - 1 of the ring. Pairs at or past `end` are not
-// evaluated.
-template <bool kBlue, bool kHybrid, bool kMulti>
-__device__ __forceinline__ void consume_pairs(const AccumulateParams& a, const FrameRng& rng,
-                                              const StreamRow* __restrict__ ring, const uint32_t window,
-                                              const uint32_t end, const uint32_t bits, const uint32_t rows_before,
-                                              const uint32_t lane) {
-    // Lanes past `end` in the last window may read a ring entry no row has written yet; the masks keep
-    // their blue-noise texel inside the slice (their REDs are predicated off).
-    constexpr uint32_t kBlueRowMask = (kBlueNoiseHeight - 1u) * kBlueNoiseWidth;
-    const uint32_t q = window + lane;
-    const uint32_t owner = rows_before + __popc(bits & (kFullMask >> (31u - lane))) - 1u;
-    const ulonglong2* r = reinterpret_cast<const ulonglong2*>(ring + (owner & (kStreamRows - 1u)));
-    const ulonglong2 w0 = r[0];
-    const ulonglong2 w1 = r[1];
-    const uint4 w2 = reinterpret_cast<const uint4*>(r)[2];
-    const uint4 w3 = reinterpret_cast<const uint4*>(r)[3];
-    const uint32_t start = w3.z & 0xffffffu;
-    const uint32_t len = w3.z >> 24;
-    const uint32_t j2 = 2u * (q - start);
-    const uint32_t x = (w3.y & ~kGatherFormFlag) + j2;
-    const float dy = __uint_as_float(w2.x);
-    const float opacity = __uint_as_float(w2.y);
-    const unsigned long long key = (static_cast<unsigned long long>(w2.w) << 32) | w2.z;
-    const float fx = static_cast<float>(x);  // pixel coordinates are exact in float
-    const bool in = q < end;
-    eval_pair<kBlue, kHybrid, kMulti>(a, rng, a.framebuffer + (static_cast<size_t>(w3.w) + j2), x,
-                                      f2_pack(fx, fx + 1.0f), w0.x, w0.y, w1.x, w1.y, f2_pack(dy, dy),
-                                      f2_pack(opacity, opacity), key, kBlue ? (w3.x & kBlueRowMask) : w3.x,
-                                      (w3.x >> 16) & (kBlueNoiseWidth - 1u), (w3.y & kGatherFormFlag) != 0, in,
-                                      in && j2 + 1u < len);
 }
 
 // Rows per chunk of a queued Gaussian of AABB width w: about kChunkPixels pixels, a power of two
@@ -319,16 +256,15 @@ __device__ __forceinline__ void walk_chunk(const AccumulateParams& a, const Fram
 
 // One thread per Gaussian (accumulate_scatter.cu:19-77 for the projection and the AABB).
 template <bool kBlue, bool kHybrid, bool kMulti>
-__global__ void __launch_bounds__(kScatterBlock, kScatterBlocksPerSM) st_scatter_kernel(const AccumulateParams a) {
-    __shared__ RowGaussian s_gauss[kScatterWarps][32];
-    __shared__ StreamRow s_ring[kScatterWarps][kStreamRows];
-    __shared__ uint32_t s_bits[kScatterWarps][kStreamWords];
+__global__ void __launch_bounds__(kBlock, 4) st_scatter_kernel(const AccumulateParams a) {
+    __shared__ RowGaussian s_gauss[kWarpsPerBlock][32];
+    __shared__ uint32_t s_rank[kWarpsPerBlock][32];
 
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t wib = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t upto_mask = kFullMask >> (31u - lane);
-    const uint32_t idx = blockIdx.x * kScatterBlock + threadIdx.x;
+    const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
     bool active = idx < a.n;
     const uint32_t g = active ? idx : a.n - 1;
 
@@ -393,30 +329,34 @@ __global__ void __launch_bounds__(kScatterBlock, kScatterBlocksPerSM) st_scatter
         }
     }
 
-    // level 1: the rows of this warp's Gaussians, end to end in lane order, 32 rows at a time. A row's
-    // owner is found as the ordinal of its Gaussian among the warp's Gaussians with rows (the count of
-    // row starts up to it), so each Gaussian's constants are stored at that ordinal
+    // level 1: the rows of this warp's Gaussians, end to end, the Gaussians ordered by their widest
+    // span so that the 32 rows walked together have similar lengths (a warp walks as long as its
+    // longest row); Gaussians without rows go last
+    uint32_t width_key = kNoRowsKey;
+    if (has_rows) {
+        uint32_t widest = G.w;
+        if (G.span.k2 > 0.0f) {
+            const float est = 2.0f * sqrtf(G.span.k2 * G.span.dymax2) + 2.0f;
+            if (est < static_cast<float>(widest)) widest = static_cast<uint32_t>(est);
+        }
+        width_key = min(widest, kNoRowsKey - 1u);
+    }
+    const uint32_t sorted = warp_sort_ascending((width_key << 5) | lane, lane);  // lane i: i-th smallest
+    const uint32_t src_lane = sorted & 31u;
+    s_rank[wib][src_lane] = lane;
     const uint32_t h = has_rows ? rect.height : 0u;
-    const uint32_t incl_rows = warp_inclusive_sum(h, lane);
-    const uint32_t total_rows = __shfl_sync(kFullMask, incl_rows, 31);
-    const uint32_t row_first = incl_rows - h;
-    const uint32_t with_rows = __ballot_sync(kFullMask, has_rows);
+    const uint32_t h_sorted = __shfl_sync(kFullMask, h, src_lane);
+    const uint32_t incl_sorted = warp_inclusive_sum(h_sorted, lane);
+    const uint32_t total_rows = __shfl_sync(kFullMask, incl_sorted, 31);
+    __syncwarp();
+    const uint32_t rank = s_rank[wib][lane];
+    const uint32_t row_first = __shfl_sync(kFullMask, incl_sorted - h_sorted, rank);
     if (has_rows) {
         RowGaussian st = G;
         st.row_first = row_first;
-        s_gauss[wib][__popc(with_rows & lt_mask)] = st;
+        s_gauss[wib][rank] = st;
     }
-    StreamRow* ring = s_ring[wib];
-    uint32_t* bitmap = s_bits[wib];
-#pragma unroll
-    for (uint32_t i = 0; i < kStreamWords / 32; ++i) bitmap[i * 32 + lane] = 0u;
     __syncwarp();
-
-    // level 2: the pixel-pair stream of the rows' spans (see the file comment)
-    uint32_t rows_head = 0;    // rows published
-    uint32_t pairs_head = 0;   // pairs published
-    uint32_t window = 0;       // first pair not yet consumed (a multiple of 32)
-    uint32_t rows_before = 0;  // rows starting before `window`
     int prev = -1;
     for (uint32_t base = 0; base < total_rows; base += 32) {
         const uint32_t rel = row_first - base;
@@ -427,58 +367,7 @@ __global__ void __launch_bounds__(kScatterBlock, kScatterBlocksPerSM) st_scatter
         const bool valid = r < total_rows;
         const RowGaussian rg = s_gauss[wib][valid ? owner : 0];
         const uint32_t y = rg.y_min + (r - rg.row_first);
-        uint32_t xs = 0, len = 0;
-        float dy = 0.0f;
-        if (valid) {
-            dy = __fsub_rn(static_cast<float>(y), rg.my);
-            row_span(rg.x_min, rg.w, rg.mx, rg.span, dy, xs, len);
-        }
-        const bool long_row = len > 2u * kStreamMaxPairs;
-        const uint32_t pairs = long_row ? 0u : (len + 1u) >> 1;
-        const uint32_t published = __ballot_sync(kFullMask, pairs != 0u);
-        const uint32_t incl_pairs = warp_inclusive_sum(pairs, lane);
-        if (pairs != 0u) {
-            const uint32_t start = pairs_head + incl_pairs - pairs;
-            uint32_t bx;
-            const uint32_t seed = row_seed<kBlue>(rng, rg.key_lo, y, bx);
-            const float cydy = __fmul_rn(rg.cy, dy);
-            const float czdy = __fmul_rn(rg.cz, dy);
-            StreamRow sr;
-            sr.mx[0] = sr.mx[1] = rg.mx;
-            sr.cx[0] = sr.cx[1] = rg.cx;
-            sr.cydy[0] = sr.cydy[1] = cydy;
-            sr.czdy[0] = sr.czdy[1] = czdy;
-            sr.dy = dy;
-            sr.opacity = rg.opacity;
-            sr.key_lo = rg.key_lo;
-            sr.key_hi = rg.key_hi;
-            sr.seed = kBlue ? (seed | (bx << 16)) : seed;
-            sr.x0 = xs | (kHybrid ? (rg.flags & kGatherFormFlag) : 0u);
-            sr.start_len = start | (len << 24);
-            sr.index = y * a.cam.width_int + xs;
-            ring[(rows_head + __popc(published & lt_mask)) & (kStreamRows - 1u)] = sr;
-            atomicOr(&bitmap[(start >> 5) & (kStreamWords - 1u)], 1u << (start & 31u));
-        }
-        rows_head += __popc(published);
-        pairs_head += __shfl_sync(kFullMask, incl_pairs, 31);
-        __syncwarp();
-        // consume every full window of 32 pairs
-        while (pairs_head - window >= 32u) {
-            const uint32_t word = (window >> 5) & (kStreamWords - 1u);
-            const uint32_t starts = bitmap[word];
-            consume_pairs<kBlue, kHybrid, kMulti>(a, rng, ring, window, pairs_head, starts, rows_before, lane);
-            rows_before += __popc(starts);
-            window += 32u;
-            __syncwarp();
-            if (lane == 0) bitmap[word] = 0u;
-        }
-        // the few rows longer than the stream takes: one row per lane
-        if (__any_sync(kFullMask, long_row)) walk_rows<kBlue, kHybrid, kMulti>(a, rng, long_row, rg, y);
-        __syncwarp();
-    }
-    if (pairs_head > window) {
-        const uint32_t starts = bitmap[(window >> 5) & (kStreamWords - 1u)];
-        consume_pairs<kBlue, kHybrid, kMulti>(a, rng, ring, window, pairs_head, starts, rows_before, lane);
+        walk_rows<kBlue, kHybrid, kMulti>(a, rng, valid, rg, y);
     }
 
     // queue overflow: the warp processes its kept large Gaussians, 32 rows at a time
@@ -566,7 +455,7 @@ __global__ void clear_kernel(unsigned long long* __restrict__ fb, const size_t n
 
 template <bool kBlue, bool kHybrid, bool kMulti>
 void launch_st(const AccumulateParams& p, const unsigned grid, const unsigned queue_grid, cudaStream_t stream) {
-    st_scatter_kernel<kBlue, kHybrid, kMulti><<<grid, kScatterBlock, 0, stream>>>(p);
+    st_scatter_kernel<kBlue, kHybrid, kMulti><<<grid, kBlock, 0, stream>>>(p);
     st_queue_kernel<kBlue, kHybrid, kMulti><<<queue_grid, kBlock, 0, stream>>>(p);
 }
 
@@ -593,7 +482,7 @@ cudaError_t launch_clear(unsigned long long* framebuffer, const size_t n_fb, Wor
 
 cudaError_t launch_accumulate_st(const AccumulateParams& p, const int num_sms, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
-    const unsigned grid = (p.n + kScatterBlock - 1) / kScatterBlock;
+    const unsigned grid = (p.n + kBlock - 1) / kBlock;
     const unsigned queue_grid = static_cast<unsigned>(num_sms) * kQueueBlocksPerSM;
     if (p.n_samples > 1) launch_st_variant<true>(p, grid, queue_grid, stream);
     else launch_st_variant<false>(p, grid, queue_grid, stream);

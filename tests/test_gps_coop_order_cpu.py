@@ -104,44 +104,3 @@ def test_buffered_schedule_fills_the_lanes():
     counts = [10] * 32  # 6 cooperative points each: 32 iterations in the reference, 6 here
     _, flushes = buffered_order(counts)
     assert flushes == 2  # 192 items in buffers of 128 (126 when the next 6 do not fit, then 66)
-
-
-def reference_own_order(counts: list[int]) -> dict:
-    """(lane, i) -> (lane, k): the reference's sequential phase, lane l drawing its own first points."""
-    return {(lane, i): (lane, i) for lane in range(32) for i in range(min(counts[lane], SEQ))}
-
-
-def parked_own_order(counts: list[int]) -> tuple[dict, int]:
-    """The kernel's own-point phase: each lane's min(count, 4) draws parked at its exclusive prefix in the
-    128-item buffer, then evaluated 32 at a time; returns (lane, i) -> (lane, k) and the item count."""
-    own = [min(c, SEQ) for c in counts]
-    buf = [None] * ITEMS
-    incl = 0
-    for lane in range(32):
-        incl += own[lane]
-        at = incl - own[lane]
-        for i in range(own[lane]):
-            assert 0 <= at + i < ITEMS and buf[at + i] is None
-            buf[at + i] = ((lane, i), (lane, i))
-    out = {}
-    for base in range(0, incl, 32):
-        for lane in range(32):
-            b = base + lane
-            if b < incl:
-                key, drawn = buf[b]
-                assert key not in out
-                out[key] = drawn
-    return out, incl
-
-
-@pytest.mark.parametrize("seed", range(10))
-def test_parked_own_points_draw_like_the_reference(seed):
-    """Every lane's first points keep their draw numbers in the lane's own stream, each is evaluated
-    once, and the 32 x 4 possible points fit the buffer."""
-    rng = random.Random(seed)
-    counts = [rng.choice([0, 1, 2, 3, 4, 5, 40]) for _ in range(32)]
-    got, n = parked_own_order(counts)
-    assert got == reference_own_order(counts)
-    assert n <= ITEMS
-    full, n_full = parked_own_order([SEQ] * 32)
-    assert n_full == ITEMS and len(full) == ITEMS

@@ -100,132 +100,34 @@ def test_segments_partition_a_span(length, log_segs):
     assert covered == list(range(xs, xs + length))
 
 
-# ---- the scatter kernel's pixel-pair stream (st_scatter_kernel, consume_pairs) ----
+# ---- the scatter kernel's level 1 (st_scatter_kernel) ----
 
-STREAM_ROWS = 64
-STREAM_WORDS = 128
-STREAM_MAX_PAIRS = 64
+NO_ROWS_KEY = (1 << 26) - 1
 
 
-def run_pair_stream(batches: list[list[tuple[int, int]]]):
-    """Restates one warp's pair stream: `batches` holds, per batch of (at most) 32 rows, each lane's row
-    span (xs, length). Returns the pixels written per (row id, x), the ids given to the published rows,
-    the rows walked lane by lane, and the largest number of live ring rows and bitmap words seen."""
-    ring: dict[int, tuple] = {}
-    bitmap = [0] * STREAM_WORDS
-    rows_head = pairs_head = window = rows_before = 0
-    written: dict[tuple[int, int], int] = {}
-    long_rows = []
-    max_live_rows = max_words = 0
-
-    def consume(end):
-        nonlocal rows_before
-        starts = bitmap[(window >> 5) & (STREAM_WORDS - 1)]
-        for lane in range(32):
-            q = window + lane
-            owner = rows_before + bin(starts & ((1 << (lane + 1)) - 1)).count("1") - 1
-            if q >= end:
-                continue
-            row_id, xs, length, start = ring[owner & (STREAM_ROWS - 1)]
-            assert row_id == owner, "a live ring entry was overwritten"
-            j2 = 2 * (q - start)
-            assert 0 <= j2 < length
-            for x in (xs + j2, xs + j2 + 1):
-                if x < xs + length:
-                    written[(row_id, x)] = written.get((row_id, x), 0) + 1
-        rows_before += bin(starts).count("1")
-
-    row_id_of = {}
-    for b, batch in enumerate(batches):
-        assert len(batch) <= 32
-        pairs = [(length + 1) // 2 if length <= 2 * STREAM_MAX_PAIRS else 0 for _, length in batch]
-        incl = rank = 0
-        for lane, ((xs, length), p) in enumerate(zip(batch, pairs)):
-            incl += p
-            if p:
-                start = pairs_head + incl - p
-                rid = rows_head + rank
-                ring[rid & (STREAM_ROWS - 1)] = (rid, xs, length, start)
-                row_id_of[(b, lane)] = rid
-                word = (start >> 5) & (STREAM_WORDS - 1)
-                assert not bitmap[word] >> (start & 31) & 1
-                bitmap[word] |= 1 << (start & 31)
-                rank += 1
-            elif length > 2 * STREAM_MAX_PAIRS:
-                long_rows.append((b, lane))
-        rows_head += rank
-        pairs_head += incl
-        max_live_rows = max(max_live_rows, rows_head - rows_before)
-        max_words = max(max_words, (pairs_head + 31) // 32 - window // 32)
-        while pairs_head - window >= 32:
-            word = (window >> 5) & (STREAM_WORDS - 1)
-            consume(pairs_head)
-            window += 32
-            bitmap[word] = 0
-    if pairs_head > window:
-        consume(pairs_head)
-    return written, row_id_of, long_rows, max_live_rows, max_words
-
-
-@pytest.mark.parametrize("seed", range(16))
-def test_pair_stream_writes_each_span_pixel_once(seed):
-    rng = random.Random(seed)
-    batches = []
-    for _ in range(rng.randint(1, 40)):
-        n = 32 if rng.random() < 0.8 else rng.randint(1, 32)
-        kind = rng.random()
-        batch = []
-        for _ in range(n):
-            if rng.random() < 0.15:
-                batch.append((0, 0))  # an empty span
-            elif kind < 0.1:
-                batch.append((rng.randint(0, 100), rng.randint(100, 300)))  # long rows, some walked by lanes
-            elif kind < 0.2:
-                batch.append((rng.randint(0, 100), 2 * STREAM_MAX_PAIRS))  # the longest streamed rows
-            else:
-                batch.append((rng.randint(0, 2000), rng.randint(1, 9)))
-        batches.append(batch)
-    written, ids, long_rows, live, words = run_pair_stream(batches)
-    want = {}
-    for b, batch in enumerate(batches):
-        for lane, (xs, length) in enumerate(batch):
-            if (b, lane) in ids:
-                for x in range(xs, xs + length):
-                    want[(ids[(b, lane)], x)] = 1
-            elif length > 0:
-                assert length > 2 * STREAM_MAX_PAIRS and (b, lane) in long_rows
-    assert written == want
-    assert live <= STREAM_ROWS and words <= STREAM_WORDS
-
-
-def test_pair_stream_capacity_bounds():
-    """Worst cases for the rings: a batch of 32 one-pair rows after 31 pending one-pair rows, and a
-    batch of 32 rows of the most pairs the stream takes."""
-    batches = [[(0, 1)] * 31, [(0, 2)] * 32, [(0, 2 * STREAM_MAX_PAIRS)] * 32, [(0, 1)] * 32]
-    _, _, _, live, words = run_pair_stream(batches)
-    assert live <= STREAM_ROWS and words <= STREAM_WORDS
-    assert live == 63
-
-
-def level1_owner_slots(heights: list[int]) -> list[tuple[int, int]]:
+def level1_owner_slots(heights: list[int], widths: list[int]) -> list[tuple[int, int]]:
     """st_scatter_kernel's level 1 for one warp: lane l's Gaussian has heights[l] AABB rows (0: culled,
-    queued or empty). Rows are laid end to end in lane order; each Gaussian with rows is stored at slot
-    popc(lanes with rows below it); a row finds its slot as `prev + popc(row starts up to it)` over
-    32-row batches. Returns, per row, (slot read, lane the slot was written by)."""
-    with_rows = [h > 0 for h in heights]
-    incl, row_first, slots = 0, [], {}
-    for lane, h in enumerate(heights):
-        row_first.append(incl)
-        incl += h
-        if with_rows[lane]:
-            slots[sum(with_rows[:lane])] = lane
+    queued or empty) of about widths[l] pixels. The Gaussians are sorted by (width, lane), those without
+    rows last; their rows are laid end to end in that order and each Gaussian with rows is stored at
+    its rank; a row finds its slot as `prev + popc(row starts up to it)` over 32-row batches. Returns,
+    per row, (slot read, lane the slot was written by)."""
+    keys = [((min(w, NO_ROWS_KEY - 1) if h > 0 else NO_ROWS_KEY) << 5) | lane
+            for lane, (h, w) in enumerate(zip(heights, widths))]
+    order = sorted(range(32), key=lambda lane: keys[lane])  # position i: the lane of the i-th smallest key
+    rank = {lane: i for i, lane in enumerate(order)}
+    incl, first_sorted = 0, []
+    for lane in order:
+        first_sorted.append(incl)
+        incl += heights[lane]
+    row_first = [first_sorted[rank[lane]] for lane in range(32)]
+    slots = {rank[lane]: lane for lane in range(32) if heights[lane] > 0}
     total = incl
     out, prev = [], -1
     for base in range(0, total, 32):
         bits = 0
         for lane in range(32):
             rel = row_first[lane] - base
-            if with_rows[lane] and 0 <= rel < 32:
+            if heights[lane] > 0 and 0 <= rel < 32:
                 bits |= 1 << rel
         for lane in range(32):
             r = base + lane
@@ -239,9 +141,12 @@ def level1_owner_slots(heights: list[int]) -> list[tuple[int, int]]:
 @pytest.mark.parametrize("seed", range(20))
 def test_level1_rows_find_their_own_gaussian(seed):
     """Every row reads the constants of the Gaussian it belongs to, also with Gaussians without rows
-    between them (a lane-indexed store would hand those rows another Gaussian's or an unwritten slot)."""
+    among them (sorted last, so the ranks of the Gaussians with rows are 0, 1, ... in row order), and
+    the rows come in order of the Gaussians' widths."""
     rng = random.Random(seed)
     heights = [0 if rng.random() < 0.4 else rng.randint(1, rng.choice([3, 40, 200])) for _ in range(32)]
-    want = [lane for lane, h in enumerate(heights) for _ in range(h)]
-    got = [lane for _, lane in level1_owner_slots(heights)]
+    widths = [rng.randint(1, rng.choice([4, 64, 3000])) for _ in range(32)]
+    order = sorted((lane for lane in range(32) if heights[lane] > 0), key=lambda lane: (widths[lane], lane))
+    want = [lane for lane in order for _ in range(heights[lane])]
+    got = [lane for _, lane in level1_owner_slots(heights, widths)]
     assert got == want
