@@ -213,7 +213,16 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
             const uint32_t full = n_items & ~31u;
             if (full != 0) {
                 const PointSource t = shfl_source(s, src);
-                for (uint32_t j = lane; j < full; j += 32) gps_point(a, fb, seed, t);
+                // Gaussians with more points than the hybrid mode's binning threshold (heavy-tailed
+                // scenes) mostly land on pixels that already hold a nearer key: their points read the
+                // key first and skip those atomics (about a quarter of the accumulate time on 1M
+                // heavy-tailed Gaussians at 1280x720 ss 2); for the many small Gaussians of other
+                // scenes the extra load costs more than it saves
+                if (n_items + kSequentialFragments > kBinningPointThreshold) {
+                    for (uint32_t j = lane; j < full; j += 32) gps_point<true>(a, fb, seed, t);
+                } else {
+                    for (uint32_t j = lane; j < full; j += 32) gps_point(a, fb, seed, t);
+                }
             }
             const uint32_t rest = n_items - full;
             if (rest == 0) continue;
