@@ -76,6 +76,46 @@ __device__ __forceinline__ void gps_point(const AccumulateParams& a, unsigned lo
     gps_point_at<kFilter>(a, fb, pcg2d_uniform(seed), s);
 }
 
+// The pixel the point drawn from uniforms `u` lands on, or null when it leaves the image or fails the
+// power test (the tests of gps_point_at).
+__device__ __forceinline__ unsigned long long* gps_point_pixel(const AccumulateParams& a,
+                                                                unsigned long long* __restrict__ fb, const float2 u,
+                                                                const PointSource& s) {
+    const float2 xy = truncated_box_muller(u.x, u.y, s.opacity_rcp, s.opacity_dilog);
+    const float sx = s.mean2d.x + s.L.x * xy.x;
+    const float sy = s.mean2d.y + (s.L.y * xy.x + s.L.z * xy.y);
+    if (sx >= a.cam.width || sx < 0.0f || sy >= a.cam.height || sy < 0.0f) return nullptr;
+    const float dcx = truncf(sx) + 0.5f - s.mean2d.x;
+    const float dcy = truncf(sy) + 0.5f - s.mean2d.y;
+    const float power = 0.5f * (s.conic.x * dcx * dcx + s.conic.z * dcy * dcy) + s.conic.y * dcx * dcy;
+    if (power > s.power_threshold) return nullptr;
+    return &fb[__float2uint_rd(sy) * a.cam.width_int + __float2uint_rd(sx)];
+}
+
+// `n` points per lane (the same n on every lane) drawn in order from the lane's stream, kGroup at a
+// time: the group's pixels first, then their keys read together (relaxed loads at GPU scope), then the
+// atomics the keys leave (the filter of gps_point_at, its loads overlapped instead of one per point).
+constexpr uint32_t kFilterGroup = 4;
+__device__ __forceinline__ void gps_points_filtered(const AccumulateParams& a, unsigned long long* __restrict__ fb,
+                                                    uint2& seed, const PointSource& s, const uint32_t n) {
+    uint32_t i = 0;
+    for (; i + kFilterGroup <= n; i += kFilterGroup) {
+        unsigned long long* pixel[kFilterGroup];
+#pragma unroll
+        for (uint32_t k = 0; k < kFilterGroup; ++k) pixel[k] = gps_point_pixel(a, fb, pcg2d_uniform(seed), s);
+        unsigned long long current[kFilterGroup];
+#pragma unroll
+        for (uint32_t k = 0; k < kFilterGroup; ++k) {
+            current[k] = 0ull;
+            if (pixel[k] != nullptr) asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(current[k]) : "l"(pixel[k]));
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kFilterGroup; ++k)
+            if (pixel[k] != nullptr && current[k] > s.key) atomicMin(pixel[k], s.key);
+    }
+    for (; i < n; ++i) gps_point<true>(a, fb, seed, s);
+}
+
 __device__ __forceinline__ PointSource shfl_source(const PointSource& s, const uint32_t src) {
     PointSource o;
     o.mean2d = make_float2(__shfl_sync(kFullMask, s.mean2d.x, src), __shfl_sync(kFullMask, s.mean2d.y, src));
@@ -111,7 +151,7 @@ __device__ __forceinline__ void evaluate_parked(const AccumulateParams& a, unsig
 // framebuffer each (scatter scheduling only). Both are template switches so that the one-sample
 // scatter kernel carries neither the frame loop nor the binning code.
 template <bool kHybrid, bool kMulti>
-__global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulateParams a) {
+__device__ __forceinline__ void gps_scatter(const AccumulateParams& a) {
     static_assert(!(kHybrid && kMulti), "several samples per call use scatter scheduling");
     __shared__ uint2 s_state[kBlock / 32][kItemsPerWarp];
     __shared__ uint8_t s_src[kBlock / 32][kItemsPerWarp];
@@ -213,13 +253,18 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
             const uint32_t full = n_items & ~31u;
             if (full != 0) {
                 const PointSource t = shfl_source(s, src);
-                // Gaussians with more points than the hybrid mode's binning threshold (heavy-tailed
-                // scenes) mostly land on pixels that already hold a nearer key: their points read the
-                // key first and skip those atomics (about a quarter of the accumulate time on 1M
-                // heavy-tailed Gaussians at 1280x720 ss 2); for the many small Gaussians of other
-                // scenes the extra load costs more than it saves
+                // Gaussians with more points than the binning threshold (heavy-tailed scenes; in hybrid
+                // mode those beyond a full bin) mostly land on pixels that already hold a nearer key:
+                // their points read the key first and skip those atomics. The hybrid kernel, which
+                // meets them by the hundred thousand with a small max_binned, reads four points' keys
+                // at a time; for the many small Gaussians of other scenes the extra loads would cost
+                // more than they save.
                 if (n_items + kSequentialFragments > kBinningPointThreshold) {
-                    for (uint32_t j = lane; j < full; j += 32) gps_point<true>(a, fb, seed, t);
+                    if (kHybrid) {
+                        gps_points_filtered(a, fb, seed, t, full / 32u);
+                    } else {
+                        for (uint32_t j = lane; j < full; j += 32) gps_point<true>(a, fb, seed, t);
+                    }
                 } else {
                     for (uint32_t j = lane; j < full; j += 32) gps_point(a, fb, seed, t);
                 }
@@ -239,6 +284,17 @@ __global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulatePar
         }
         if (fill != 0) evaluate_parked(a, fb, s, s_state[warp], s_src[warp], fill, lane);
     }
+}
+
+template <bool kMulti>
+__global__ void __launch_bounds__(kBlock) gps_scatter_kernel(const AccumulateParams a) {
+    gps_scatter<false, kMulti>(a);
+}
+
+// The hybrid kernel carries the key filter of overflowing large Gaussians; held to 5 resident blocks
+// per SM (at most 51 registers, no spills) like the plain kernel's 47-48 registers give.
+__global__ void __launch_bounds__(kBlock, 5) gps_scatter_hybrid_kernel(const AccumulateParams a) {
+    gps_scatter<true, false>(a);
 }
 
 // Persistent consumer of the binned Gaussians: each warp steals kChunksPerClaim 256-point chunks at
@@ -303,9 +359,9 @@ __global__ void __launch_bounds__(kBlock, kQueueBlocksPerSM) gps_queue_kernel(co
 cudaError_t launch_accumulate_gps(const AccumulateParams& p, const int num_sms, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
     const unsigned grid = (p.n + kBlock - 1) / kBlock;
-    if (p.hybrid) gps_scatter_kernel<true, false><<<grid, kBlock, 0, stream>>>(p);
-    else if (p.n_samples > 1) gps_scatter_kernel<false, true><<<grid, kBlock, 0, stream>>>(p);
-    else gps_scatter_kernel<false, false><<<grid, kBlock, 0, stream>>>(p);
+    if (p.hybrid) gps_scatter_hybrid_kernel<<<grid, kBlock, 0, stream>>>(p);
+    else if (p.n_samples > 1) gps_scatter_kernel<true><<<grid, kBlock, 0, stream>>>(p);
+    else gps_scatter_kernel<false><<<grid, kBlock, 0, stream>>>(p);
     if (p.hybrid) gps_queue_kernel<<<static_cast<unsigned>(num_sms) * kQueueBlocksPerSM, kBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }
