@@ -475,6 +475,11 @@ def run_ours(args, world, rank, local) -> dict | None:
             "stochastic_transparency": reference_cuda_baseline(scene, cam, dict(fl, gps=False), dev),
             "gps": reference_cuda_baseline(scene, cam, dict(fl, gps=True), dev),
         }
+        # the small-scene configuration (100k Gaussians at 640x480), where the per-call host work of
+        # the bindings weighs as much as the kernels
+        s_c0, cam_c0, fl_c0 = make_inputs("st_100k_640_st")
+        line["reference_cuda"]["c0_st_100k_640"] = reference_cuda_baseline(s_c0.to(dev), cam_c0, fl_c0, dev, calls=64)
+        del s_c0
     if not (args.no_train and args.no_learned) and args.workload.startswith("batch_6m"):
         del scene
         torch.cuda.empty_cache()
