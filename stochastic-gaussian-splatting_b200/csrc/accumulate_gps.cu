@@ -164,7 +164,8 @@ __device__ __forceinline__ void gps_scatter(const AccumulateParams& a) {
     Projected p;
     if (!project_gaussian(active, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, a.pre, a.quant)) return;
 
-    // importance and number of points (accumulate_scatter.cu:104-112)
+    // expected point count from the truncated footprint's area and opacity, then its Poisson draw
+    // (accumulate_scatter.cu:104-112)
     PointSource s;
     s.opacity_dilog = gps_dilog(p.opacity);
     const float importance = kTwoPi * sqrtf(p.determinant) * s.opacity_dilog;

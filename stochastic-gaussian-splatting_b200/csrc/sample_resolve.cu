@@ -112,13 +112,14 @@ __global__ void __launch_bounds__(kBlock) reuse_sample_kernel(const ResolveParam
     const float4 sample = warp_sample(a, data, threadIdx.x & 31u);
     if (active) a.samples[pixel] = sample;
 
-    // the winner projected again, to evaluate it at the neighbours
+    // alpha of this subpixel's winner at the subpixel and at its four neighbours needs its 2-D conic again
     bool projected = active && has_sample;
     Projected p;
     project_gaussian(projected, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, nullptr, a.quant);
     if (!active) return;
 
-    // weights start with the change in alpha; background counts as opaque and farthest
+    // per-neighbour weight = neighbour alpha over own alpha; a subpixel without a winner behaves as an
+    // opaque surface at infinite depth
     float alpha = 1.0f;
     float4 na = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     float sample_depth = __uint_as_float(0x7f800000u);
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(kBlock) reuse_sample_kernel(const ResolveParam
     float4 occl[kKBufferSize];
 #pragma unroll
     for (uint32_t k = 0; k < kKBufferSize; ++k) {
-        // entries of empty slots hold a NaN depth, which never compares below
+        // an unused slot's depth bits are a NaN, so the depth test below is false for it
         const bool occludes = __uint_as_float(prims[k].y) < sample_depth;
         occl[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (occludes || (unique && k + 1u < kKBufferSize)) occl[k] = a.k_occl[static_cast<size_t>(k) * a.n_fb + pixel];
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(kBlock) reuse_sample_kernel(const ResolveParam
             weights.w *= occl[k].w;
         }
     }
-    // a new primitive enters at the front and the last entry drops out
+    // a winner not yet in the k-buffer shifts the entries down one slot (the last is lost) and takes slot 0
     if (unique) {
 #pragma unroll
         for (uint32_t k = kKBufferSize - 1; k > 0; --k) {
@@ -372,7 +373,7 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
     float depth = ds, alpha = as, weight_mass = ws;
     if constexpr (!kReproject) {
         if (a.temporal_mode == 1 && active) {
-            // weighted cumulative moving average (resolve.cu:250-258)
+            // Static: merge with the history weighted by the accumulated weight mass (resolve.cu:250-258)
             const float hm = a.hist_weight_mass[pixel];
             weight_mass = hm + ws;
             const float hf = hm / weight_mass;
@@ -407,7 +408,8 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
             }
         }
 
-        // reproject the sampled surface point, background at the far plane (resolve.cu:261-283)
+        // where this pixel's sampled surface was in the previous view: mean winner depth of the valid
+        // subpixels, the far plane where none is valid (resolve.cu:261-283)
         const float z = valid > 0 ? depth_out / static_cast<float>(valid) : a.far_plane;
         const float fpx = static_cast<float>(px) + 0.5f;
         const float fpy = static_cast<float>(py) + 0.5f;
@@ -421,7 +423,8 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
         if (use_history) {
             ppx = a.focal_x * (m1.x * vx + m1.y * vy + m1.z * vz + m1.w) / pz + a.center_x;
             ppy = a.focal_y * (m2.x * vx + m2.y * vy + m2.z * vz + m2.w) / pz + a.center_y;
-            // no history near the border, which keeps every Catmull-Rom tap inside the image
+            // points within the margin of the image edge take no history, so the 4 x 4 taps below never
+            // leave the image
             use_history = ppx >= kBorderMargin && ppx <= static_cast<float>(a.width) - kBorderMargin &&
                           ppy >= kBorderMargin && ppy <= static_cast<float>(a.height) - kBorderMargin;
         }
@@ -469,7 +472,8 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
         }
 
         if (use_history) {
-            // Catmull-Rom history fetch without clamping (resolve.cu:285-305)
+            // bicubic (Catmull-Rom) filter of the previous outputs around that point, unclamped
+            // (resolve.cu:285-305)
             const float4 wx4 = catmull_rom_weights(tx - tbx);
             const float4 wy4 = catmull_rom_weights(ty - tby);
             const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
@@ -508,7 +512,8 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
                 }
             }
 
-            // YCoCg moments of the current samples in the 3 x 3 window (resolve.cu:307-326)
+            // mean and mean square, in YCoCg, of this sample's box-filtered colours over the pixel and its 8
+            // neighbours (clamped at the edges) (resolve.cu:307-326)
             float3 mean = make_float3(0.0f, 0.0f, 0.0f);
             float3 mean_sq = make_float3(0.0f, 0.0f, 0.0f);
             for (int wy = -1; wy <= 1; ++wy) {
@@ -540,8 +545,9 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
             const float sdy = sqrtf(fmaxf(mean_sq.y - mean.y * mean.y, 0.0f));
             const float sdz = sqrtf(fmaxf(mean_sq.z - mean.z * mean.z, 0.0f));
 
-            // soft rejection of the history; confidence half-extents shrink with the pixel's motion
-            // (resolve.cu:328-339)
+            // how far the history colour lies outside a box of gamma standard deviations around the mean
+            // (gamma falls from the static to the moving value as the pixel moves faster), as a
+            // discount of the history weight (resolve.cu:328-339)
             const float dvx = fpx - ppx, dvy = fpy - ppy;
             const float velocity = sqrtf(dvx * dvx + dvy * dvy);
             const float gamma = kGammaStatic + fminf(velocity / kVelocityThreshold, 1.0f) * (kGammaMotion - kGammaStatic);
@@ -559,7 +565,8 @@ __global__ void __launch_bounds__(kBlock) tile_resolve_kernel(const ResolveParam
             color.z = cs.z + discount * (ch.z - cs.z);
             depth = ds + discount * (dh - ds);
             alpha = as + discount * (ah - as);
-            // the weight mass the blend would settle at, used once the camera stops
+            // weight mass of a sum that kept this discount forever: Static merges start from it when the
+            // view stops moving
             weight_mass = ws / (1.0f - discount);
         }
     }
