@@ -203,8 +203,8 @@ int sgs_render_no_alloc(const sgs_gaussians* gaussians, const sgs_camera* camera
  *      `weight` = the sample's weight in the averaged output (1/S for a plain progressive average);
  *      `first` = 1 for the first sample (clears the accumulators);
  *   2. sgs_backward_finish writes the parameter gradients (overwriting them).
- * Supported: stochastic transparency (white or blue noise, scatter or hybrid), any supersampling,
- * Reset/Static; not GPS, spatial reuse or proper antialiasing (SGS_ERROR_INVALID_ARGUMENT).
+ * Supported: stochastic transparency (white or blue noise, scatter or hybrid), any supersampling, with
+ * or without proper antialiasing, Reset/Static; not GPS or spatial reuse (SGS_ERROR_INVALID_ARGUMENT).
  * `backward_workspace` holds sgs_backward_workspace_size(n) bytes, 16-byte aligned. */
 size_t sgs_backward_workspace_size(uint32_t n_gaussians);
 int sgs_backward_accumulate(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,

@@ -151,15 +151,16 @@ def _f64(a) -> np.ndarray:
 
 
 def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None, g_image=None, g_alpha=None,
-                   g_depth=None, grad: bool = False) -> dict:
+                   g_depth=None, grad: bool = False, aa: bool = False) -> dict:
     """Expected image of one stochastic-transparency sample (double precision) and, with `grad`, the
     gradient of sum(g_image * image + g_alpha * alpha + g_depth * depth) w.r.t. every parameter.
-    The fragment support and key order are frozen at `base` (single precision; default: `scene`)."""
+    The fragment support and key order are frozen at `base` (single precision; default: `scene`).
+    `aa`: proper antialiasing (smaller dilation, opacity scaled by sqrt(det / det dilated))."""
     l = lib()
     if not hasattr(l.oracle_expected_image, "_typed"):
         P, u, d, i = _P, ctypes.c_uint32, ctypes.c_double, ctypes.c_int
-        l.oracle_expected_image.argtypes = [P, P, P, P, P, u, u, P, P, u, u, d, d, d, d, d, d, i, P, P, P, P, P, P, P,
-                                            P, P, P, P, P, P, P, P, P]
+        l.oracle_expected_image.argtypes = [P, P, P, P, P, u, u, P, P, u, u, d, d, d, d, d, d, i, i, P, P, P, P, P, P,
+                                            P, P, P, P, P, P, P, P, P, P]
         l.oracle_expected_image._typed = True
     base = scene if base is None else base
     m, s, r, o, sh = (_f64(scene[k]) for k in ("means", "scales", "rotations", "opacities", "sh_coefficients"))
@@ -180,7 +181,8 @@ def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None
     w2c = _f64(np.asarray(cam["w2c"])[:3].reshape(-1))
     l.oracle_expected_image(_p(m), _p(s), _p(r), _p(o), _p(sh), n, bases, _p(w2c), _p(_f64(cam["position"])), W, H,
                             cam["focal_x"], cam["focal_y"], cam["center_x"], cam["center_y"], cam["near_plane"],
-                            cam["far_plane"], int(ss), _p(bm), _p(bs), _p(br), _p(bo), _p(gi), _p(ga), _p(gd),
+                            cam["far_plane"], int(ss), int(aa), _p(bm), _p(bs), _p(br), _p(bo), _p(gi), _p(ga),
+                            _p(gd),
                             _p(image), _p(alpha), _p(depth), ctypes.byref(loss),
                             *(_p(out[k]) if grad else None for k in ("means", "scales", "rotations", "opacities",
                                                                      "sh_coefficients")))

@@ -827,7 +827,11 @@ struct ProjD {
     double qn[4], qnorm;
     double R[3][3], v[3], S[3][3], T[2][3];
     double a, b, c, det, conic[3];
-    double op, m2[2];
+    double sig;             // sigmoid of the opacity logit
+    double raw_xx, raw_yy;  // diagonal of the undilated 2-D covariance
+    double det_raw, ratio;  // proper antialiasing: det of the undilated covariance, det_raw / det
+    bool aa;
+    double op, m2[2];       // op: the opacity alpha uses (sig, times sqrt(ratio) with antialiasing)
     double dvec[3], dlen, dir[3], color[3], Y[16];
     bool cpos[3];
 };
@@ -857,7 +861,7 @@ void sh_basis(const double x, const double y, const double z, double Y[16], doub
 
 ProjD project_d(const double* m, const double* s, const double* q, const double o, const double* sh, uint32_t bases,
                 const double* W, const double* cam, const double fx, const double fy, const double cx0,
-                const double cy0, const double width, const double height, const double dil) {
+                const double cy0, const double width, const double height, const double dil, const bool aa) {
     ProjD p{};
     for (int r = 0; r < 3; ++r) p.t[r] = W[4 * r] * m[0] + W[4 * r + 1] * m[1] + W[4 * r + 2] * m[2] + W[4 * r + 3];
     p.x = p.t[0] / p.t[2];
@@ -904,7 +908,15 @@ ProjD project_d(const double* m, const double* s, const double* q, const double 
     p.conic[0] = p.c / p.det;
     p.conic[1] = -p.b / p.det;
     p.conic[2] = p.a / p.det;
-    p.op = 1.0 / (1.0 + std::exp(-o));
+    p.sig = 1.0 / (1.0 + std::exp(-o));
+    // proper antialiasing keeps the integral of the dilated footprint: opacity * sqrt(det / det dilated)
+    // (gs_utils.h:155,165-166)
+    p.aa = aa;
+    p.raw_xx = cov[0][0];
+    p.raw_yy = cov[1][1];
+    p.det_raw = cov[0][0] * cov[1][1] - cov[0][1] * cov[0][1];
+    p.ratio = p.det_raw / p.det;
+    p.op = aa ? p.sig * std::sqrt(std::max(p.ratio, 0.0)) : p.sig;
     p.m2[0] = p.x * fx + cx0;
     p.m2[1] = p.y * fy + cy0;
     for (int i = 0; i < 3; ++i) p.dvec[i] = m[i] - cam[i];
@@ -930,7 +942,8 @@ struct GradProj {
 void project_d_backward(const ProjD& p, const GradProj& g, const double* sh, uint32_t bases, const double* W,
                         const double fx, const double fy, double* dm, double* ds, double* dq, double* dopac,
                         double* dsh) {
-    *dopac = g.op * p.op * (1.0 - p.op);
+    const double f = p.aa ? std::sqrt(std::max(p.ratio, 0.0)) : 1.0;
+    *dopac = g.op * f * p.sig * (1.0 - p.sig);
     // conic = inverse(cov2d + dilation): dL/dcov = -C G C
     const double C[2][2] = {{p.conic[0], p.conic[1]}, {p.conic[1], p.conic[2]}};
     const double G[2][2] = {{g.conic[0], 0.5 * g.conic[1]}, {0.5 * g.conic[1], g.conic[2]}};
@@ -939,6 +952,16 @@ void project_d_backward(const ProjD& p, const GradProj& g, const double* sh, uin
         for (int j = 0; j < 2; ++j) CG[i][j] = C[i][0] * G[0][j] + C[i][1] * G[1][j];
     for (int i = 0; i < 2; ++i)
         for (int j = 0; j < 2; ++j) GA[i][j] = -(CG[i][0] * C[0][j] + CG[i][1] * C[1][j]);
+    if (p.aa && p.ratio > 0.0) {
+        // op = sig sqrt(r), r = det_raw / det with det_raw = xx yy - xy^2 and det = (xx + d)(yy + d) - xy^2
+        // dL/dr = g.op sig / (2 sqrt(r)); dr/dxx = (yy det - det_raw (yy + d)) / det^2, likewise for yy,
+        // dr/dxy = 2 xy (det_raw - det) / det^2, split over the two off-diagonal entries
+        const double k = g.op * p.sig / (2.0 * f) / (p.det * p.det);
+        GA[0][0] += k * (p.raw_yy * p.det - p.det_raw * p.c);
+        GA[1][1] += k * (p.raw_xx * p.det - p.det_raw * p.a);
+        GA[0][1] += k * (p.b * (p.det_raw - p.det));
+        GA[1][0] += k * (p.b * (p.det_raw - p.det));
+    }
     // G_cov symmetric with off-diagonal dL/db / 2 = GA[0][1]
     double dS[3][3], dT[2][3];
     for (int i = 0; i < 3; ++i)
@@ -1025,7 +1048,7 @@ extern "C" {
 int oracle_expected_image(const double* means, const double* scales, const double* rotations, const double* opacities,
                           const double* sh, uint32_t n, uint32_t bases, const double* w2c, const double* cam_pos,
                           uint32_t width, uint32_t height, double fx, double fy, double cx, double cy, double near_plane,
-                          double far_plane, int ss_raw, const float* base_means, const float* base_scales,
+                          double far_plane, int ss_raw, int aa, const float* base_means, const float* base_scales,
                           const float* base_rotations, const float* base_opacities, const double* g_image,
                           const double* g_alpha, const double* g_depth, double* image, double* alpha, double* depth,
                           double* loss, double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
@@ -1034,11 +1057,11 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
     float w2cf[12];
     for (int i = 0; i < 12; ++i) w2cf[i] = static_cast<float>(w2c[i]);
     const Cam cam = make_cam(width, height, static_cast<float>(fx), static_cast<float>(fy), static_cast<float>(cx),
-                             static_cast<float>(cy), static_cast<float>(near_plane), static_cast<float>(far_plane), 0,
+                             static_cast<float>(cy), static_cast<float>(near_plane), static_cast<float>(far_plane), aa,
                              static_cast<int>(ss));
     const uint32_t fbw = width * ss, fbh = height * ss;
     const double dfx = fx * ss, dfy = fy * ss, dcx = cx * ss, dcy = cy * ss;
-    const double dil = kDilation * ss * ss;
+    const double dil = (aa ? kDilationAA : kDilation) * ss * ss;
     // frozen support and order from the single-precision forward
     std::vector<std::vector<std::pair<uint64_t, uint32_t>>> frags(static_cast<size_t>(fbw) * fbh);
     for (uint32_t g = 0; g < n; ++g) {
@@ -1056,7 +1079,8 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
     std::vector<ProjD> pd(n);
     for (uint32_t g = 0; g < n; ++g)
         pd[g] = project_d(means + 3 * g, scales + 3 * g, rotations + 4 * g, opacities[g], sh + static_cast<size_t>(g) * bases * 3,
-                          bases, w2c, cam_pos, dfx, dfy, dcx, dcy, static_cast<double>(fbw), static_cast<double>(fbh), dil);
+                          bases, w2c, cam_pos, dfx, dfy, dcx, dcy, static_cast<double>(fbw), static_cast<double>(fbh), dil,
+                          aa != 0);
     const bool grad = d_means != nullptr;
     std::vector<GradProj> gp(grad ? n : 0);
     for (auto& x : gp) x = GradProj{};

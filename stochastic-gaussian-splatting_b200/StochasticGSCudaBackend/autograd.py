@@ -69,9 +69,8 @@ def _render_all(tensors, settings: Settings, n_samples: int, first_frame: int):
 class _RenderSamples(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means, scales, rotations, opacities, sh, settings, n_samples, first_frame, store_winners):
-        if settings.use_gps or settings.spatial_reuse or settings.proper_antialiasing:
-            raise RuntimeError("render_samples differentiates stochastic transparency without spatial reuse or "
-                               "proper antialiasing")
+        if settings.use_gps or settings.spatial_reuse:
+            raise RuntimeError("render_samples differentiates stochastic transparency without spatial reuse")
         tensors = tuple(t.detach().contiguous() for t in (means, scales, rotations, opacities, sh))
         (image, depth, alpha, _), ws, layout = _render_all(tensors, settings, n_samples, first_frame)
         ctx.save_for_backward(*tensors)

@@ -18,10 +18,9 @@ struct BackwardSetup {
 
 int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, BackwardSetup& out) {
     if (g == nullptr || c == nullptr || s == nullptr) return record_error(SGS_ERROR_INVALID_ARGUMENT, "null argument");
-    if (s->use_gps || s->spatial_reuse || s->proper_antialiasing)
+    if (s->use_gps || s->spatial_reuse)
         return record_error(SGS_ERROR_INVALID_ARGUMENT,
-                            "the backward pass supports stochastic transparency without spatial reuse or proper "
-                            "antialiasing");
+                            "the backward pass supports stochastic transparency without spatial reuse");
     if (g->sh_bases != 1 && g->sh_bases != 4 && g->sh_bases != 9 && g->sh_bases != 16)
         return record_error(SGS_ERROR_INVALID_ARGUMENT, "sh_bases must be 1, 4, 9 or 16");
     if (g->quantized != nullptr)
@@ -55,7 +54,7 @@ int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, Ba
     p.cam.far_plane = c->far_plane;
     p.cam.ss = ssf;
     p.cam.width_int = c->width * ss;
-    p.cam.proper_aa = false;
+    p.cam.proper_aa = s->proper_antialiasing;
     p.width = c->width;
     p.ss = ss;
     p.n_fb = c->width * ss * c->height * ss;

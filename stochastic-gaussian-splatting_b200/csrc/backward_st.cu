@@ -539,14 +539,19 @@ __global__ void __launch_bounds__(kBlock) projection_backward_kernel(const Backw
                 for (int l = 0; l < 3; ++l) s += T[i][k] * S[k][l] * T[j][l];
             cov[i][j] = s;
         }
-    const float dil = kDilation * cam.ss * cam.ss;
+    const float dil = (cam.proper_aa ? kDilationProperAA : kDilation) * cam.ss * cam.ss;
     const float a = cov[0][0] + dil, bb = cov[0][1], c = cov[1][1] + dil;
     const float det = a * c - bb * bb;
     const float C[2][2] = {{c / det, -bb / det}, {-bb / det, a / det}};
     const float op = 1.0f / (1.0f + expf(-b.opacities[g]));
+    // proper antialiasing scales the opacity by f = sqrt(det_raw / det), det_raw of the undilated
+    // covariance (gs_utils.h:165-166); acc[0] is the gradient w.r.t. that scaled opacity
+    const float det_raw = cov[0][0] * cov[1][1] - cov[0][1] * cov[0][1];
+    const float ratio = det_raw / det;
+    const float f = cam.proper_aa ? sqrtf(fmaxf(ratio, 0.0f)) : 1.0f;
 
     // opacity logit
-    b.d_opacities[g] = acc[0] * op * (1.0f - op);
+    b.d_opacities[g] = acc[0] * f * op * (1.0f - op);
     // conic = inverse(cov2d + dilation)
     const float G[2][2] = {{acc[1], 0.5f * acc[2]}, {0.5f * acc[2], acc[3]}};
     float CG[2][2], GA[2][2];
@@ -554,6 +559,15 @@ __global__ void __launch_bounds__(kBlock) projection_backward_kernel(const Backw
         for (int j = 0; j < 2; ++j) CG[i][j] = C[i][0] * G[0][j] + C[i][1] * G[1][j];
     for (int i = 0; i < 2; ++i)
         for (int j = 0; j < 2; ++j) GA[i][j] = -(CG[i][0] * C[0][j] + CG[i][1] * C[1][j]);
+    if (cam.proper_aa && ratio > 0.0f) {
+        // f through the covariance: dr/dxx = (yy det - det_raw (yy + d)) / det^2 (likewise yy) and
+        // dr/dxy = 2 xy (det_raw - det) / det^2, split over the two off-diagonal entries
+        const float k = acc[0] * op / (2.0f * f) / (det * det);
+        GA[0][0] += k * (cov[1][1] * det - det_raw * c);
+        GA[1][1] += k * (cov[0][0] * det - det_raw * a);
+        GA[0][1] += k * (bb * (det_raw - det));
+        GA[1][0] += k * (bb * (det_raw - det));
+    }
     float dS[3][3], dT[2][3];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {

@@ -1,6 +1,7 @@
 """The analytic gradient of the expected image (the backward's checker) against central finite
 differences (eps 1e-3) on 64 sampled parameters (CPU)."""
 import numpy as np
+import pytest
 
 import sgs_scenes
 from oracle import cpu
@@ -36,10 +37,25 @@ def test_expected_image_matches_the_monte_carlo_mean_of_the_oracle():
     assert err.mean() < 0.01 and np.percentile(err, 99) < 0.08
 
 
-def test_analytic_gradient_matches_central_differences():
+def test_expected_image_matches_the_monte_carlo_mean_with_antialiasing():
+    """The same check with proper antialiasing (opacity scaled by sqrt(det / det dilated))."""
+    scene, cd, *_ = _setup()
+    exp = cpu.expected_image(scene, cd, aa=True)
+    flags = dict(aa=True, ss=1, gps=False, hybrid=False)
+    acc = np.zeros((36, 48, 3))
+    n = 600
+    for f in range(n):
+        fb = cpu.accumulate(scene, cd, flags, f, threads=2)
+        acc += cpu.sample_resolve(scene, cd, flags, fb, threads=2)["image"]
+    err = np.abs(acc / n - exp["image"])
+    assert err.mean() < 0.01 and np.percentile(err, 99) < 0.08
+
+
+@pytest.mark.parametrize("aa", [False, True])
+def test_analytic_gradient_matches_central_differences(aa):
     scene, cd, gi, ga, gd = _setup()
     base = {k: v.copy() for k, v in scene.items()}
-    res = cpu.expected_image(scene, cd, base=base, g_image=gi, g_alpha=ga, g_depth=gd, grad=True)
+    res = cpu.expected_image(scene, cd, base=base, g_image=gi, g_alpha=ga, g_depth=gd, grad=True, aa=aa)
     rng = np.random.default_rng(1)
     eps = 1e-3
     checked = 0
@@ -51,8 +67,8 @@ def test_analytic_gradient_matches_central_differences():
             minus = {kk: vv.astype(np.float64).copy() for kk, vv in scene.items()}
             plus[k].reshape(-1)[idx] += eps
             minus[k].reshape(-1)[idx] -= eps
-            lp = cpu.expected_image(plus, cd, base=base, g_image=gi, g_alpha=ga, g_depth=gd)["loss"]
-            lm = cpu.expected_image(minus, cd, base=base, g_image=gi, g_alpha=ga, g_depth=gd)["loss"]
+            lp = cpu.expected_image(plus, cd, base=base, g_image=gi, g_alpha=ga, g_depth=gd, aa=aa)["loss"]
+            lm = cpu.expected_image(minus, cd, base=base, g_image=gi, g_alpha=ga, g_depth=gd, aa=aa)["loss"]
             fd = (lp - lm) / (2 * eps)
             an = res["grad"][k].reshape(-1)[idx]
             worst.append((abs(fd - an) / max(1e-3, abs(fd)), k, idx, fd, an))

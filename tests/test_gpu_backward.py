@@ -38,15 +38,19 @@ def _settings(cam, ss):
                     cam.near_plane, cam.far_plane, False, ss, False, False, False)
 
 
-@pytest.mark.parametrize("ss,hybrid,store", [(1, False, True), (2, False, False), (1, True, True)])
-def test_estimator_matches_exact_gradient(ss, hybrid, store, cuda_device):
+@pytest.mark.parametrize("ss,hybrid,store,aa", [(1, False, True, False), (2, False, False, False),
+                                                 (1, True, True, False), (1, False, True, True),
+                                                 (2, False, False, True)])
+def test_estimator_matches_exact_gradient(ss, hybrid, store, aa, cuda_device):
+    """Also with proper antialiasing (aa): the opacity scaled by sqrt(det / det dilated) and the smaller
+    dilation, through both the per-fragment terms and the projection backward."""
     scene, cam, gi, ga, gd = _problem(ss)
     sc = {k: t.numpy() for k, t in zip(KEYS, scene.tensors())}
     cd = dict(width=W, height=H, focal_x=cam.focal_x, focal_y=cam.focal_y, center_x=cam.center_x,
               center_y=cam.center_y, near_plane=cam.near_plane, far_plane=cam.far_plane, w2c=cam.w2c.numpy(),
               position=cam.position.numpy())
-    exact = cpu.expected_image(sc, cd, ss=ss, g_image=gi, g_alpha=ga, g_depth=gd, grad=True)["grad"]
-    settings = _settings(cam, ss)._replace(hybrid_scheduling=hybrid)
+    exact = cpu.expected_image(sc, cd, ss=ss, g_image=gi, g_alpha=ga, g_depth=gd, grad=True, aa=aa)["grad"]
+    settings = _settings(cam, ss)._replace(hybrid_scheduling=hybrid, proper_antialiasing=aa)
     gi_t = torch.tensor(gi, dtype=torch.float32, device="cuda")
     ga_t = torch.tensor(ga, dtype=torch.float32, device="cuda")
     gd_t = torch.tensor(gd, dtype=torch.float32, device="cuda")
