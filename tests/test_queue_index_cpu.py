@@ -5,7 +5,9 @@ by the whole warp; `gps_queue_kernel` (csrc/accumulate_gps.cu) claims 8 chunks p
 the entry only when a chunk lies past it. These tests run the same steps lane by lane in Python on
 random and edge-case queues and check that every chunk maps to its owner (the last entry whose first
 chunk is <= c), that every index a lane reads is in bounds, and that the claims draw every point of
-every entry exactly once.
+every entry exactly once. An entry whose chunks would pass 32-bit chunk indices is marked unused by its
+producer (csrc/accumulate_gps.cu, accumulate_st.cu, backward_st.cu); the last test restates that
+marking and the consumers' search for the last used entry.
 """
 import random
 
@@ -115,3 +117,58 @@ def test_claims_draw_every_point_once(seed):
     assert all(len(d) == n for d, n in zip(drawn, counts))
     # the cursor overshoots the last chunk by less than one claim per warp
     assert cursor - n_chunks < warps * CHUNKS_PER_CLAIM + CHUNKS_PER_CLAIM
+
+
+UNUSED = 0xFFFFFFFF
+MAX_QUEUE_CHUNKS = 0xFFFFFFFF - (1 << 24)
+
+
+def reserve(chunks_per_entry: list[int], capacity: int, start_chunk: int = 0):
+    """The producers' reservations in arrival order (entry index and first chunk from one 64-bit word):
+    an entry whose chunks would pass MAX_QUEUE_CHUNKS is marked unused (first chunk UNUSED, no points)
+    and its Gaussian scattered instead. Returns the queue's first-chunk array, point counts and the
+    entries kept."""
+    first, count, kept = [], [], []
+    total = start_chunk
+    for e, ch in enumerate(chunks_per_entry):
+        if e >= capacity:
+            total += ch
+            continue
+        if total + ch <= MAX_QUEUE_CHUNKS:
+            first.append(total)
+            count.append(ch * CHUNK_POINTS)
+            kept.append(e)
+        else:
+            first.append(UNUSED)
+            count.append(0)
+        total += ch
+    return first, count, kept
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_marked_entries_are_the_last_ones_and_the_consumer_ends_at_the_last_used(seed):
+    """With the chunk counter near the 32-bit limit (a first entry that starts late stands in for the
+    chunks of earlier entries), the marked entries form the queue's tail, the consumer's last used entry
+    is found by the same search (marked entries start past every chunk), and every chunk below the
+    consumer's total maps to a used entry."""
+    rng = random.Random(seed)
+    chunks = [rng.choice([3, 4, 1800, 7201, 16200]) for _ in range(400)]
+    # entry 0 starts at chunk 0; let the later ones start close to the limit
+    big = MAX_QUEUE_CHUNKS - sum(chunks[1:200])
+    chunks[0] = big
+    first, count, kept = reserve(chunks, capacity=300)
+    n_entries = min(len(chunks), 300)
+    assert first[0] == 0
+    marked = [e for e in range(n_entries) if first[e] == UNUSED]
+    assert marked and marked == list(range(marked[0], n_entries))
+    last = n_entries - 1
+    if first[last] == UNUSED:
+        last = entry_of_chunk(first, n_entries, UNUSED - 1)
+    assert last == max(kept)
+    n_chunks = first[last] + (count[last] + CHUNK_POINTS - 1) // CHUNK_POINTS
+    assert n_chunks <= MAX_QUEUE_CHUNKS
+    for c in {0, n_chunks - 1, first[last], big - 1, big} | {rng.randrange(n_chunks) for _ in range(100)}:
+        if c >= n_chunks:
+            continue
+        e = entry_of_chunk(first, n_entries, c)
+        assert first[e] != UNUSED and first[e] <= c < first[e] + count[e] // CHUNK_POINTS
