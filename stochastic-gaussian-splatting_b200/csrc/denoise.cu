@@ -147,7 +147,10 @@ __device__ __forceinline__ void load_accumulator(uint32_t taddr, float (&acc)[N]
 
 // Epilogue of one output pixel (thread m of the tile owns pixel m = 8 * row + column): bias and
 // ReLU, bias and residual (final layer), or the ReLU mask of the layer below (data gradient).
-template <int COUT, int EPI>
+// kPlanar: the BF16 output is stored as 8-channel planes [batch][channel / 8][y][x][8] (the layout of
+// the denoiser's internal activations: a warp's store covers 128 contiguous bytes per tile row, and a
+// halo box of one plane is a 160-byte run per row) instead of NHWC.
+template <int COUT, int EPI, bool kPlanar = false>
 __device__ __forceinline__ void store_pixel(const ConvArgs& a, const TileXY& tile, int m, const float (&acc)[COUT],
                                             const float (&bias)[COUT]) {
     const int x = tile.x0 + (m & 7), y = tile.y0 + (m >> 3);
@@ -162,7 +165,11 @@ __device__ __forceinline__ void store_pixel(const ConvArgs& a, const TileXY& til
         out[1] = acc[1] + bias[1] + rg.y;
         out[2] = acc[2] + bias[2] + bx.x;
     } else {
-        uint4* out = static_cast<uint4*>(a.out) + pixel * (COUT / 8);
+        const size_t plane = static_cast<size_t>(a.height) * a.width;
+        const size_t first = kPlanar ? (static_cast<size_t>(tile.b) * (COUT / 8) * plane + static_cast<size_t>(y) * a.width + x)
+                                     : pixel * (COUT / 8);
+        const size_t step = kPlanar ? plane : 1;
+        uint4* out = static_cast<uint4*>(a.out) + first;
 #pragma unroll
         for (int q = 0; q < COUT / 8; ++q) {
             float v[8];
@@ -180,13 +187,13 @@ __device__ __forceinline__ void store_pixel(const ConvArgs& a, const TileXY& til
                     if (!(bf16_hi(mw[i]) > 0.0f)) v[2 * i + 1] = 0.0f;
                 }
             }
-            out[q] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
-                                pack_bf16(v[6], v[7]));
+            out[q * step] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                                       pack_bf16(v[6], v[7]));
         }
     }
 }
 
-template <int CIN, int COUT, int IN, int EPI>
+template <int CIN, int COUT, int IN, int EPI, bool kPlanar = false>
 __global__ void __launch_bounds__(kThreads, 1) conv3x3_kernel(const ConvArgs a) {
     constexpr int KC = CIN / 8;
     constexpr int kWeightVecs = 9 * KC * COUT;
@@ -246,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_kernel(const ConvArgs a) 
         float acc[COUT];
         load_accumulator<COUT>(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
 
-        if (ok) store_pixel<COUT, EPI>(a, tile, tid, acc, bias);
+        if (ok) store_pixel<COUT, EPI, kPlanar>(a, tile, tid, acc, bias);
         tc::fence_before_sync();
         if (__syncthreads_or(!ok)) {
             failed = true;
@@ -290,7 +297,9 @@ struct TmaConv {
     static_assert((kChunkPx * 16) % 128 == 0 && (kWeightVecs * 16) % 128 == 0, "128-byte TMA destinations");
 };
 
-template <int CIN, int COUT, int EPI>
+// kPlanar: input and BF16 output in the 8-channel-plane layout of store_pixel (the tensor map is then
+// over [batch][plane][y][x * 8 + channel] and a chunk's halo is one box of 10 x 18 pixels).
+template <int CIN, int COUT, int EPI, bool kPlanar = false>
 __global__ void __launch_bounds__(kTmaThreads, 1) conv3x3_tma_kernel(const __grid_constant__ CUtensorMap in_map,
                                                                   const ConvArgs a) {
     using S = TmaConv<CIN, COUT>;
@@ -343,9 +352,13 @@ __global__ void __launch_bounds__(kTmaThreads, 1) conv3x3_tma_kernel(const __gri
                 const TileXY tile = tile_xy(t, a.tiles_x, a.tiles_y);
                 tc::mbar_arrive_expect_tx(SGS_FULL(st), S::kTxBytes);
 #pragma unroll
-                for (int c = 0; c < S::KC; ++c)
-                    tc::tma_load_4d(halo_a + (st * S::kHaloVecs + c * S::kChunkPx) * 16, &in_map, SGS_FULL(st), c * 8,
-                                    tile.x0 - 1, tile.y0 - 1, tile.b);
+                for (int c = 0; c < S::KC; ++c) {
+                    const uint32_t dst = halo_a + (st * S::kHaloVecs + c * S::kChunkPx) * 16;
+                    if constexpr (kPlanar)  // x in elements: 8 per pixel, so always a 16-byte multiple
+                        tc::tma_load_4d(dst, &in_map, SGS_FULL(st), (tile.x0 - 1) * 8, tile.y0 - 1, c, tile.b);
+                    else
+                        tc::tma_load_4d(dst, &in_map, SGS_FULL(st), c * 8, tile.x0 - 1, tile.y0 - 1, tile.b);
+                }
             }
         }
     } else if (warp == 5) {
@@ -392,7 +405,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) conv3x3_tma_kernel(const __gri
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(SGS_ACC_EMPTY(k));
-            store_pixel<COUT, EPI>(a, tile_xy(t, a.tiles_x, a.tiles_y), tid, acc, bias);
+            store_pixel<COUT, EPI, kPlanar>(a, tile_xy(t, a.tiles_x, a.tiles_y), tid, acc, bias);
         }
     }
 
@@ -623,10 +636,10 @@ int resident_ctas(Kernel kernel, size_t smem, int cap, int threads = kThreads) {
     return blocks < cap ? blocks : cap;
 }
 
-template <int CIN, int COUT, int IN, int EPI>
+template <int CIN, int COUT, int IN, int EPI, bool kPlanar = false>
 cudaError_t launch_conv(const ConvArgs& a, cudaStream_t stream) {
     constexpr size_t smem = static_cast<size_t>(9 * (CIN / 8) * COUT + (CIN / 8) * kHaloPx) * 16 + 16;
-    auto kernel = conv3x3_kernel<CIN, COUT, IN, EPI>;
+    auto kernel = conv3x3_kernel<CIN, COUT, IN, EPI, kPlanar>;
     static const int per_sm = resident_ctas(kernel, smem, 8);
     if (per_sm <= 0) return cudaErrorInvalidConfiguration;
     const int grid = a.n_tiles < sm_count() * per_sm ? a.n_tiles : sm_count() * per_sm;
@@ -665,14 +678,33 @@ bool nhwc_halo_map(CUtensorMap* map, const void* base, int batch, int height, in
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int CIN, int COUT, int EPI>
+// The same halo boxes over activations in 8-channel planes, [batch][channels / 8][y][x][8]: dimension 0
+// runs over x * 8 + channel, so a plane's box is 10 pixels (160 bytes) wide and 18 rows high.
+bool planar_halo_map(CUtensorMap* map, const void* base, int batch, int height, int width, int channels) {
+    const auto fn = encode_tiled();
+    if (fn == nullptr) return false;
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(width) * 8, static_cast<cuuint64_t>(height),
+                                static_cast<cuuint64_t>(channels / 8), static_cast<cuuint64_t>(batch)};
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(width) * 16,
+                                   static_cast<cuuint64_t>(height) * width * 16,
+                                   static_cast<cuuint64_t>(channels / 8) * height * width * 16};
+    const cuuint32_t box[4] = {kHaloW * 8, kHaloH, 1, 1};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, elem,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int CIN, int COUT, int EPI, bool kPlanar = false>
 cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t stream) {
     using S = TmaConv<CIN, COUT>;
-    auto kernel = conv3x3_tma_kernel<CIN, COUT, EPI>;
+    auto kernel = conv3x3_tma_kernel<CIN, COUT, EPI, kPlanar>;
     static const int per_sm = resident_ctas(kernel, S::kSmem, 512 / kTmaCols, kTmaThreads);
     if (per_sm <= 0) return cudaErrorInvalidConfiguration;
     CUtensorMap map;
-    if (!nhwc_halo_map(&map, a.in, a.batch, a.height, a.width, CIN)) return cudaErrorInvalidValue;
+    const bool mapped = kPlanar ? planar_halo_map(&map, a.in, a.batch, a.height, a.width, CIN)
+                                : nhwc_halo_map(&map, a.in, a.batch, a.height, a.width, CIN);
+    if (!mapped) return cudaErrorInvalidValue;
     const int grid = a.n_tiles < sm_count() * per_sm ? a.n_tiles : sm_count() * per_sm;
     kernel<<<grid, kTmaThreads, S::kSmem, stream>>>(map, a);
     return cudaGetLastError();
@@ -836,24 +868,30 @@ int sgs_denoise(const void* features, int32_t batch, int32_t height, int32_t wid
     if (scratch_bytes < sgs_denoise_scratch_size(batch, height, width) || !aligned16(scratch))
         return record_error(SGS_ERROR_WORKSPACE, "denoise: scratch needs %zu bytes, 16-byte aligned",
                             sgs_denoise_scratch_size(batch, height, width));
+    if (!aligned16(features) || !aligned16(weights))
+        return record_error(SGS_ERROR_INVALID_ARGUMENT, "denoise: features and weights must be 16-byte aligned");
+    // the hidden activations live only in the scratch, so they use the 8-channel-plane layout (wider
+    // halo boxes, coalesced stores); the same arithmetic as the NHWC layers of sgs_conv3x3
     unsigned char* act[2] = {static_cast<unsigned char*>(scratch),
                              static_cast<unsigned char*>(scratch) + sgs_denoise_scratch_size(batch, height, width) / 2};
     const unsigned char* w = static_cast<const unsigned char*>(weights);
     const float* b = biases;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const int tiles_x = (width + kTileW - 1) / kTileW, tiles_y = (height + kTileH - 1) / kTileH;
     for (int l = 0; l < kLayers; ++l) {
-        sgs_conv3x3_args c{};
-        c.input = l == 0 ? features : act[(l + 1) & 1];
-        c.output = l == kLayers - 1 ? static_cast<void*>(output) : act[l & 1];
-        c.weights = w;
-        c.bias = b;
-        c.residual = l == kLayers - 1 ? features : nullptr;
-        c.batch = batch;
-        c.height = height;
-        c.width = width;
-        c.in_channels = kLayerIn[l];
-        c.out_channels = kLayerOut[l];
-        c.epilogue = l == kLayers - 1 ? SGS_CONV_FINAL : SGS_CONV_RELU;
-        if (int st = sgs_conv3x3(&c, stream_ptr)) return st;
+        const bool last = l == kLayers - 1;
+        ConvArgs a{l == 0 ? features : act[(l + 1) & 1], last ? static_cast<void*>(output) : act[l & 1],
+                   reinterpret_cast<const uint4*>(w), b, nullptr,
+                   last ? static_cast<const uint4*>(features) : nullptr, batch, height, width, tiles_x, tiles_y, 0};
+        a.n_tiles = batch * tiles_x * tiles_y;
+        cudaError_t err;
+        if (l == 0)
+            err = launch_conv<16, 32, kInFeatures, kEpiRelu, true>(a, stream);
+        else if (!last)
+            err = launch_conv_tma<32, 32, kEpiRelu, true>(a, stream);
+        else
+            err = launch_conv_tma<32, 16, kEpiFinal, true>(a, stream);
+        if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "denoise layer %d: %s", l + 1, cudaGetErrorString(err));
         w += weights_bytes(kLayerIn[l], kLayerOut[l]);
         b += kLayerOut[l];
     }
