@@ -115,7 +115,10 @@ __global__ void __launch_bounds__(kBlock) reuse_sample_kernel(const ResolveParam
     // alpha of this subpixel's winner at the subpixel and at its four neighbours needs its 2-D conic again
     bool projected = active && has_sample;
     Projected p;
-    project_gaussian(projected, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, nullptr, a.quant);
+    // lanes without a winner project Gaussian 0 alongside the others (the call is warp-collective);
+    // a warp without any winner skips it, so an empty scene reads no Gaussian at all
+    if (__any_sync(0xffffffffu, projected))
+        project_gaussian(projected, g, a.means, a.scales, a.rotations, a.opacities, a.w2c, a.cam, p, nullptr, a.quant);
     if (!active) return;
 
     // per-neighbour weight = neighbour alpha over own alpha; a subpixel without a winner behaves as an
