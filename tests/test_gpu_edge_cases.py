@@ -137,3 +137,58 @@ def test_frames_at_the_32_bit_wrap(ref, frame, cuda_device):
         got = render_once(sc, cd, flags, frame, blue_noise=blue if use_blue else None)["fb"]
         assert (want != -1).any()
         assert_bitwise(f"frame {frame:#x} gps {gps} hybrid {hybrid} blue {use_blue}", got, want)
+
+
+def _extreme_scene(dev):
+    """Duplicated Gaussians (equal depth keys, the index decides) and extreme parameters: opacity logits
+    of +-12, log-scales from -7 (sub-pixel) to +1 (covering the image), means straddling the near plane."""
+    base = sgs_scenes.make_scene(sgs_scenes.SceneSpec(n=3000, log_scale_mean=-2.5, log_scale_std=1.5), 21)
+    g = torch.Generator().manual_seed(22)
+    m, s, r, o, sh = (t.clone() for t in base.tensors())
+    o[:300] = 12.0
+    o[300:600] = -12.0
+    s[600:700] = -7.0
+    s[700:720] = 1.0
+    m[720:800, 2] = -4.0 + 0.2 + torch.rand(80, generator=g) * 0.01  # near the camera's near plane (z = -4 + 0.2)
+    dup = slice(800, 1400)
+    m2, s2, r2, o2, sh2 = (torch.cat([t, t[dup]]) for t in (m, s, r, o, sh))
+    return sgs_scenes.Scene(m2, s2, r2, o2, sh2).to(dev)
+
+
+@pytest.mark.parametrize("gps,hybrid", [(False, False), (False, True), (True, False), (True, True)])
+def test_collisions_and_extreme_parameters_bitwise(ref, gps, hybrid, cuda_device):
+    """Equal depth keys resolve to the lower index and extreme opacities, scales and near-plane means are
+    culled, clamped and binned as the reference does: outputs and k-buffer bitwise over Reset, Static and
+    Reproject with spatial reuse (supersampling 2)."""
+    from StochasticGSCudaBackend import _C
+
+    ref_C, _ = ref
+    dev = cuda_device
+    scene = _extreme_scene(dev)
+    width, height, ss = 96, 64, 2
+    cams = sgs_scenes.orbit_cameras(8, 4.0, width, height, step_deg=4.0)
+    n_fb = width * height * ss * ss
+    kb_ref = (torch.full((4, n_fb, 2), -1, dtype=torch.int32, device=dev), torch.zeros((4, n_fb, 4), device=dev))
+    kb_our = (kb_ref[0].clone(), kb_ref[1].clone())
+    e = torch.empty(0)
+    h_ref = h_our = (e, e, e, e)
+    prev = cams[0]
+    for i, mode in enumerate((0, 1, 2, 1)):
+        cam = cams[1] if i >= 2 else cams[0]
+        v2pv = (prev.w2c.double() @ torch.linalg.inv(cam.w2c.double())).float() if mode == 2 else torch.eye(4)
+
+        def args(kb, h):
+            return (*scene.tensors(), cam.w2c.to(dev), cam.position.to(dev), width, height, cam.focal_x, cam.focal_y,
+                    cam.center_x, cam.center_y, cam.near_plane, cam.far_plane, False, ss, gps, hybrid, True,
+                    torch.empty(0, dtype=torch.uint8, device=dev), *kb, *h, v2pv.to(dev), mode)
+
+        frame, h_ref = reference_render(ref_C, *args(kb_ref, h_ref))
+        _C.set_frame_index(frame)
+        h_our = _C.render(*args(kb_our, h_our))
+        torch.cuda.synchronize()
+        tag = f"gps {gps} hybrid {hybrid} step {i}"
+        for name, a, b in zip(("image", "depth", "alpha", "weight_mass"), h_our, h_ref):
+            assert_bitwise(f"{tag} {name}", a.cpu().numpy(), b.cpu().numpy())
+        assert_bitwise(f"{tag} k-buffer entries", kb_our[0].cpu().numpy(), kb_ref[0].cpu().numpy())
+        prev = cam
+    assert float(h_our[2].mean()) > 0.05
