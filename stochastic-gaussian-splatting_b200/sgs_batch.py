@@ -14,9 +14,30 @@ no copy merges a replay's outputs into the next replay's inputs.
 """
 from __future__ import annotations
 
+import contextlib
+import gc
+
 import torch
 
 from StochasticGSCudaBackend import _C
+
+
+@contextlib.contextmanager
+def graph_capture(graph: torch.cuda.CUDAGraph, **kwargs):
+    """`torch.cuda.graph(graph)` with Python's cyclic garbage collector kept out of the capture.
+
+    Garbage left to the collector (a dropped renderer's graphs, pinned buffers, events) is finalised
+    before the capture begins; during it the collector is off, so no finaliser releases CUDA
+    resources inside the capture, which would invalidate it or abort the process."""
+    gc.collect()
+    enabled = gc.isenabled()
+    gc.disable()
+    try:
+        with torch.cuda.graph(graph, **kwargs):
+            yield
+    finally:
+        if enabled:
+            gc.enable()
 
 
 class CapturedViews:
@@ -94,7 +115,7 @@ class CapturedViews:
             self.graphs = []
             for src, dst in ((0, 1), (1, 0)):
                 graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(graph):
+                with graph_capture(graph):
                     self._step_on_streams(src, dst)
                 self.graphs.append(graph)
             self.parity = 0

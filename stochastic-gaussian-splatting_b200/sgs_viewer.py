@@ -28,6 +28,7 @@ from __future__ import annotations
 import json
 import struct
 import time
+import weakref
 import zlib
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -36,6 +37,7 @@ import numpy as np
 import torch
 
 from StochasticGSCudaBackend import History, Settings, TemporalMode, _C, create_k_buffer, render
+from sgs_batch import graph_capture
 
 
 @dataclass
@@ -195,7 +197,10 @@ class _FrameGraphs:
 
     def __init__(self, renderer: "ProgressiveRenderer", settings: Settings, n_samples: int):
         dev = renderer.device
-        self.r = renderer
+        # a weak reference: the renderer owns these graphs, and without a cycle between the two they
+        # are released as soon as the renderer is, never later by the cyclic garbage collector (which
+        # may run while another renderer is capturing a graph)
+        self.r = weakref.proxy(renderer)
         self.n = n_samples
         self.settings = settings
         h, w = settings.height, settings.width
@@ -251,7 +256,7 @@ class _FrameGraphs:
             self._body(mode, parity, scratch)
             torch.cuda.synchronize(self.r.device)
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph):
+            with graph_capture(graph):
                 self.params.copy_(self.staging[parity], non_blocking=True)
                 self.counter.copy_(self.staging_frame[parity], non_blocking=True)
                 self._body(mode, parity, k_buffer)

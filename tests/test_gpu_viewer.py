@@ -82,6 +82,37 @@ def test_progressive_renderer_equals_the_sample_loop(flags, spp, graphs, cuda_de
             assert torch.equal(x[k], y[k]), f"frame {i} {k}"
 
 
+def test_dropped_renderer_releases_its_graphs_at_once(cuda_device):
+    """The frame graphs hold their renderer weakly: with the cyclic collector off, dropping a renderer
+    releases its captured graphs immediately (none is left for a collection that might run while
+    another renderer captures), and the next renderer's captures and frames work."""
+    import gc
+    import weakref
+
+    import sgs_viewer
+
+    scene = sgs_scenes.make_scene(sgs_scenes.SceneSpec(n=5_000, log_scale_mean=-3.5), seed=12)
+    model = tuple(t.cuda() for t in scene.tensors())
+    views = _views(sgs_viewer)
+    enabled = gc.isenabled()
+    gc.collect()
+    gc.disable()
+    try:
+        first = sgs_viewer.ProgressiveRenderer(*model, samples_per_pixel=1, graphs=True, temporal_reuse=True)
+        for v in views[:3]:
+            first.render_image(v)
+        frames = weakref.ref(first._frames)
+        assert len(first._frames.graphs) == 3
+        del first
+        assert frames() is None
+        second = sgs_viewer.ProgressiveRenderer(*model, samples_per_pixel=1, graphs=True, temporal_reuse=True)
+        got = [second.render_image(v)["alpha"].clone() for v in views[:3]]
+    finally:
+        if enabled:
+            gc.enable()
+    assert all(bool(torch.isfinite(a).all()) for a in got) and float(got[-1].mean()) > 0.0
+
+
 def test_composite_equals_the_tensor_operations(cuda_device):
     """_C.composite (one kernel) against the plugin's tensor operations (Renderer.py:91-97), bit for bit,
     with alphas below 0, above 1 and at 0."""
