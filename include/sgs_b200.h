@@ -204,7 +204,8 @@ int sgs_render_no_alloc(const sgs_gaussians* gaussians, const sgs_camera* camera
  *      `first` = 1 for the first sample (clears the accumulators);
  *   2. sgs_backward_finish writes the parameter gradients (overwriting them).
  * Supported: stochastic transparency (white or blue noise, scatter or hybrid), any supersampling, with
- * or without proper antialiasing, Reset/Static; not GPS or spatial reuse (SGS_ERROR_INVALID_ARGUMENT).
+ * or without proper antialiasing, Reset/Static; not spatial reuse (SGS_ERROR_INVALID_ARGUMENT). GPS
+ * gradients are computed by the fused form below only (this call rejects GPS settings).
  * `backward_workspace` holds sgs_backward_workspace_size(n) bytes, 16-byte aligned. */
 size_t sgs_backward_workspace_size(uint32_t n_gaussians);
 int sgs_backward_accumulate(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
@@ -223,9 +224,13 @@ int sgs_backward_finish(const sgs_gaussians* gaussians, const sgs_camera* camera
  *      the next sample once this call is enqueued;
  *   b. sgs_backward_accumulate_samples: the walk; `first` = 1 clears the accumulators.
  * `scratch` holds sgs_backward_samples_scratch_size(camera, settings, S) bytes (12 bytes per
- * framebuffer pixel and sample, plus 8 per pixel), 256-byte aligned; S is at most 1024. The samples'
- * terms must be written in order s = 0, 1, ..., S - 1. Same estimator, supported
- * settings and sgs_backward_finish as above. */
+ * framebuffer pixel and sample, plus 8 per pixel, plus sgs_gps_count_law_size() with GPS), 256-byte
+ * aligned; S is at most 1024. The samples' terms must be written in order s = 0, 1, ..., S - 1. Same
+ * estimator and sgs_backward_finish as above; also Gaussian point splatting (scatter or hybrid
+ * scheduling), where each fragment's alpha is replaced by the probability that the Gaussian puts a
+ * point into the (sub)pixel: 1 - E[(1 - q)^N], q the share of the Gaussian's point density over the
+ * pixel (a 3 x 3 Gauss-Legendre rule), N the point count the render draws (its law tabulated per
+ * call in the scratch). */
 size_t sgs_backward_samples_scratch_size(const sgs_camera* camera, const sgs_settings* settings, uint32_t n_samples);
 int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
                               const void* render_workspace, const float* grad_image, const float* grad_alpha,
@@ -246,6 +251,12 @@ int sgs_backward_accumulate_framebuffers(const sgs_gaussians* gaussians, const s
                                          const float* grad_image, const float* grad_alpha, const float* grad_depth,
                                          float weight, int first, void* scratch, void* backward_workspace,
                                          void* stream);
+
+/* The GPS backward's table of the point count's law (for inspection; the fused walk builds its own):
+ * 1025 rows for lambda = 2^(-10 + 13 r / 1024), 32 (P(N = n), dP/dlambda) float pairs each, the last
+ * term holding N >= 31. `out` holds sgs_gps_count_law_size() bytes, 8-byte aligned. */
+size_t sgs_gps_count_law_size(void);
+int sgs_gps_count_law(void* out, void* stream);
 
 /* ---- Learned resolve (no counterpart in the reference) ------------------------------------------
  * A 6-layer 3x3 convolutional denoiser (8 -> 32 -> 32 -> 32 -> 32 -> 32 -> 3, ReLU between layers,

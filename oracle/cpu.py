@@ -151,17 +151,21 @@ def _f64(a) -> np.ndarray:
 
 
 def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None, g_image=None, g_alpha=None,
-                   g_depth=None, grad: bool = False, aa: bool = False) -> dict:
+                   g_depth=None, grad: bool = False, aa: bool = False, gps: bool = False, quad: int = 8) -> dict:
     """Expected image of one stochastic-transparency sample (double precision) and, with `grad`, the
     gradient of sum(g_image * image + g_alpha * alpha + g_depth * depth) w.r.t. every parameter.
     The fragment support and key order are frozen at `base` (single precision; default: `scene`).
-    `aa`: proper antialiasing (smaller dilation, opacity scaled by sqrt(det / det dilated))."""
+    `aa`: proper antialiasing (smaller dilation, opacity scaled by sqrt(det / det dilated)).
+    `gps`: Gaussian point splatting instead, each fragment's alpha replaced by the probability that
+    the Gaussian puts a point into the (sub)pixel, its pixel integrals by an order-`quad`
+    Gauss-Legendre rule per axis."""
     l = lib()
+    P, u, d, i = _P, ctypes.c_uint32, ctypes.c_double, ctypes.c_int
+    args = [P, P, P, P, P, u, u, P, P, u, u, d, d, d, d, d, d, i, i, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P]
     if not hasattr(l.oracle_expected_image, "_typed"):
-        P, u, d, i = _P, ctypes.c_uint32, ctypes.c_double, ctypes.c_int
-        l.oracle_expected_image.argtypes = [P, P, P, P, P, u, u, P, P, u, u, d, d, d, d, d, d, i, i, P, P, P, P, P, P,
-                                            P, P, P, P, P, P, P, P, P, P]
+        l.oracle_expected_image.argtypes = args
         l.oracle_expected_image._typed = True
+        l.oracle_expected_image_gps.argtypes = args + [i]
     base = scene if base is None else base
     m, s, r, o, sh = (_f64(scene[k]) for k in ("means", "scales", "rotations", "opacities", "sh_coefficients"))
     bm, bs, br, bo = (_f32(base[k]) for k in ("means", "scales", "rotations", "opacities"))
@@ -179,11 +183,27 @@ def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None
         out = {"means": np.zeros_like(m), "scales": np.zeros_like(s), "rotations": np.zeros_like(r),
                "opacities": np.zeros_like(o), "sh_coefficients": np.zeros_like(sh)}
     w2c = _f64(np.asarray(cam["w2c"])[:3].reshape(-1))
-    l.oracle_expected_image(_p(m), _p(s), _p(r), _p(o), _p(sh), n, bases, _p(w2c), _p(_f64(cam["position"])), W, H,
-                            cam["focal_x"], cam["focal_y"], cam["center_x"], cam["center_y"], cam["near_plane"],
-                            cam["far_plane"], int(ss), int(aa), _p(bm), _p(bs), _p(br), _p(bo), _p(gi), _p(ga),
-                            _p(gd),
-                            _p(image), _p(alpha), _p(depth), ctypes.byref(loss),
-                            *(_p(out[k]) if grad else None for k in ("means", "scales", "rotations", "opacities",
-                                                                     "sh_coefficients")))
+    call = (_p(m), _p(s), _p(r), _p(o), _p(sh), n, bases, _p(w2c), _p(_f64(cam["position"])), W, H, cam["focal_x"],
+            cam["focal_y"], cam["center_x"], cam["center_y"], cam["near_plane"], cam["far_plane"], int(ss), int(aa),
+            _p(bm), _p(bs), _p(br), _p(bo), _p(gi), _p(ga), _p(gd), _p(image), _p(alpha), _p(depth),
+            ctypes.byref(loss),
+            *(_p(out[k]) if grad else None for k in ("means", "scales", "rotations", "opacities", "sh_coefficients")))
+    if gps:
+        l.oracle_expected_image_gps(*call, int(quad))
+    else:
+        l.oracle_expected_image(*call)
     return {"image": image, "alpha": alpha, "depth": depth, "loss": loss.value, "grad": out if grad else None}
+
+
+def gps_count_law(lam: float, cap: int = 4096) -> tuple[np.ndarray, np.ndarray]:
+    """Law of the GPS point count at importance `lam` (the Cornish-Fisher draw of the render, exact up
+    to its rounding): (P(N = n), dP(N = n) / dlam) for n = 0, 1, ..."""
+    l = lib()
+    if not hasattr(l.oracle_gps_count_law, "_typed"):
+        l.oracle_gps_count_law.argtypes = [ctypes.c_double, _P, _P, ctypes.c_int]
+        l.oracle_gps_count_law.restype = ctypes.c_int
+        l.oracle_gps_count_law._typed = True
+    P = np.zeros(cap)
+    dP = np.zeros(cap)
+    k = l.oracle_gps_count_law(float(lam), _p(P), _p(dP), cap)
+    return P[:min(k, cap)], dP[:min(k, cap)]

@@ -1037,9 +1037,247 @@ void project_d_backward(const ProjD& p, const GradProj& g, const double* sh, uin
     for (int k = 0; k < 3; ++k) dm[k] += (ddir[k] - p.dir[k] * dd) / p.dlen;
 }
 
+// ---- Gaussian point splatting: the probability that a Gaussian puts a point into a pixel ----------
+//
+// A Gaussian with projected opacity o, dilated 2-D covariance Sigma and mean m draws N points with
+// N = rint(max(kf(w), 0)), w standard normal and kf the Cornish-Fisher expansion of a Poisson
+// quantile (math_utils.h:98-111) at lambda = 2 pi sqrt(det Sigma) Li2(o) (accumulate_scatter.cu:
+// 104-112). The points are independent with density -ln(1 - o G(x)) / lambda, G(x) =
+// exp(-(x - m)^T Sigma^-1 (x - m) / 2): truncated_box_muller draws o G with P(o G <= t) =
+// Li2(t) / Li2(o) (math_utils.h:14-43 approximate Li2 and its inverse). A point in the square of
+// (sub)pixel p registers when p's centre passes the power test, so p is hit with probability
+//   h = 1 - E[(1 - q)^N],  q = Lambda_p / lambda,  Lambda_p = integral over p of -ln(1 - o G),
+// independently of every other Gaussian (for a Poisson N, h = 1 - exp(-Lambda_p)). The expected
+// image is the stochastic-transparency one with alpha replaced by h.
+
+double li2(const double x) {
+    if (x <= 0.0) return 0.0;
+    if (x >= 1.0) return 1.6449340668482264;
+    if (x > 0.5) return 1.6449340668482264 - std::log(x) * std::log1p(-x) - li2(1.0 - x);
+    double term = x, sum = 0.0;
+    for (int k = 1; k < 200 && term > 1e-18; ++k, term *= x) sum += term / (static_cast<double>(k) * k);
+    return sum;
+}
+
+// kf(w) of the count draw, and its partial derivatives in w and lambda
+double cf_kf(const double w, const double lam) {
+    const double s = std::sqrt(lam), w2 = w * w;
+    return lam + s * w + (w2 - 1.0) / 6.0 + (-(w / 36.0) - w2 * w / 72.0) / s +
+           (-(8.0 / 405.0) + (7.0 / 810.0) * w2 + w2 * w2 / 270.0) / lam;
+}
+double cf_kf_w(const double w, const double lam) {
+    const double s = std::sqrt(lam), w2 = w * w;
+    return s + w / 3.0 + (-(1.0 / 36.0) - w2 / 24.0) / s + ((14.0 / 810.0) * w + (4.0 / 270.0) * w2 * w) / lam;
+}
+double cf_kf_lam(const double w, const double lam) {
+    const double s = std::sqrt(lam), w2 = w * w;
+    return 1.0 + w / (2.0 * s) - 0.5 * (-(w / 36.0) - w2 * w / 72.0) / (lam * s) -
+           (-(8.0 / 405.0) + (7.0 / 810.0) * w2 + w2 * w2 / 270.0) / (lam * lam);
+}
+
+double normal_cdf(const double x) { return 0.5 * std::erfc(-x / std::sqrt(2.0)); }
+double normal_pdf(const double x) { return std::exp(-0.5 * x * x) / std::sqrt(2.0 * 3.14159265358979323846); }
+
+// Law of the point count: P[n] = P(N = n) and dP[n] = dP(N = n) / dlambda, n = 0 .. until the rest
+// is below 1e-15. F(t) = P(kf(w) < t) is a sum over the monotone pieces of the quartic kf on
+// [-12, 12] (outside, kf exceeds every threshold used); its lambda-derivative is
+// -sum over the roots r of kf = t of phi(r) (dkf/dlambda)(r) / |dkf/dw(r)|.
+struct CountLaw {
+    std::vector<double> P, dP;
+};
+
+CountLaw cf_count_law(const double lam) {
+    constexpr double kW = 12.0;
+    constexpr int kGrid = 4800;
+    std::vector<double> cut{-kW};
+    double prev = cf_kf_w(-kW, lam);
+    for (int i = 1; i <= kGrid; ++i) {
+        const double w = -kW + 2.0 * kW * i / kGrid;
+        const double cur = cf_kf_w(w, lam);
+        if ((prev < 0.0) != (cur < 0.0) && i < kGrid) {
+            double lo = w - 2.0 * kW / kGrid, hi = w;
+            for (int it = 0; it < 200 && hi - lo > 1e-15; ++it) {
+                const double mid = 0.5 * (lo + hi);
+                if ((cf_kf_w(mid, lam) < 0.0) == (cf_kf_w(lo, lam) < 0.0)) lo = mid;
+                else hi = mid;
+            }
+            cut.push_back(0.5 * (lo + hi));
+        }
+        prev = cur;
+    }
+    cut.push_back(kW);
+    double top = 0.0;
+    for (const double c : cut) top = std::max(top, cf_kf(c, lam));
+    // F(t) and dF/dlambda at threshold t
+    auto F = [&](const double t, double& dF) {
+        double f = 0.0;
+        dF = 0.0;
+        for (size_t i = 0; i + 1 < cut.size(); ++i) {
+            const double a = cut[i], b = cut[i + 1], fa = cf_kf(a, lam), fb = cf_kf(b, lam);
+            const bool up = fb >= fa;
+            const double lo_v = up ? fa : fb, hi_v = up ? fb : fa;
+            if (t <= lo_v) continue;
+            if (t >= hi_v) {
+                f += normal_cdf(b) - normal_cdf(a);
+                continue;
+            }
+            double lo = a, hi = b;
+            for (int it = 0; it < 200 && hi - lo > 1e-15; ++it) {
+                const double mid = 0.5 * (lo + hi);
+                if ((cf_kf(mid, lam) < t) == up) lo = mid;
+                else hi = mid;
+            }
+            const double r = 0.5 * (lo + hi);
+            f += up ? normal_cdf(r) - normal_cdf(a) : normal_cdf(b) - normal_cdf(r);
+            const double slope = std::fabs(cf_kf_w(r, lam));
+            if (slope > 0.0) dF -= normal_pdf(r) * cf_kf_lam(r, lam) / slope;
+        }
+        return f;
+    };
+    CountLaw law;
+    double f_prev = 0.0, d_prev = 0.0;
+    for (int n = 0;; ++n) {
+        double d;
+        const double f = F(n + 0.5, d);
+        law.P.push_back(f - f_prev);
+        law.dP.push_back(d - d_prev);
+        f_prev = f;
+        d_prev = d;
+        if (1.0 - f < 1e-15 || n + 0.5 > top) break;
+    }
+    return law;
+}
+
+// Gauss-Legendre nodes and weights of order n on [0, 1] (Newton on the Legendre recurrence).
+void gauss_legendre01(const int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(3.14159265358979323846 * (i + 0.75) / (n + 0.5)), dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                const double p2 = p1;
+                p1 = p0;
+                p0 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p2) / j;
+            }
+            dp = n * (z * p0 - p1) / (z * z - 1.0);
+            const double dz = p0 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        x[i] = 0.5 * (1.0 - z);
+        w[i] = 1.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// Probability of one fragment (ST alpha or GPS hit probability) and its partial derivatives in the
+// projected opacity, the conic (x, y, z) and the 2-D mean.
+struct FragP {
+    double p, d_op, d_conic[3], d_m2[2];
+};
+
+FragP st_fragment(const ProjD& p, const double px, const double py) {
+    const double dx = px - (p.m2[0] - 0.5), dy = py - (p.m2[1] - 0.5);
+    const double e = -0.5 * (p.conic[0] * dx * dx + p.conic[2] * dy * dy) - p.conic[1] * dx * dy;
+    const double a = p.op * std::exp(std::min(e, 0.0));
+    FragP f;
+    f.p = a;
+    f.d_op = a / p.op;
+    f.d_conic[0] = a * (-0.5 * dx * dx);
+    f.d_conic[1] = a * (-dx * dy);
+    f.d_conic[2] = a * (-0.5 * dy * dy);
+    f.d_m2[0] = a * (p.conic[0] * dx + p.conic[1] * dy);
+    f.d_m2[1] = a * (p.conic[1] * dx + p.conic[2] * dy);
+    return f;
+}
+
+// Per-Gaussian constants of the GPS hit probability: lambda, its derivatives in (op, conic x/y/z)
+// and the law of the count (above kPoissonLambda the count is taken as Poisson, which the
+// Cornish-Fisher draw matches to about 1e-5 there).
+struct GpsLaw {
+    double lam, d_lam[4];
+    bool poisson;
+    CountLaw law;
+};
+constexpr double kOraclePoissonLambda = 32.0;
+
+GpsLaw gps_law(const ProjD& p) {
+    GpsLaw g;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    const double sd = std::sqrt(p.det);
+    g.lam = two_pi * sd * li2(p.op);
+    const double D = p.conic[0] * p.conic[2] - p.conic[1] * p.conic[1];  // 1 / det
+    g.d_lam[0] = two_pi * sd * (-std::log1p(-std::min(p.op, 1.0 - 1e-16)) / p.op);
+    g.d_lam[1] = g.lam * (-0.5) * p.conic[2] / D;
+    g.d_lam[2] = g.lam * p.conic[1] / D;
+    g.d_lam[3] = g.lam * (-0.5) * p.conic[0] / D;
+    g.poisson = g.lam >= kOraclePoissonLambda;
+    if (!g.poisson) g.law = cf_count_law(g.lam);
+    return g;
+}
+
+// GPS hit probability of the pixel square [px, px + 1) x [py, py + 1): Lambda_p by an order-`quad`
+// Gauss-Legendre rule per axis, then h and the chain through Lambda_p and lambda.
+FragP gps_fragment(const ProjD& p, const GpsLaw& g, const double px, const double py, const std::vector<double>& qx,
+                   const std::vector<double>& qw) {
+    double Lp = 0.0, dL_op = 0.0, dL_c[3] = {0, 0, 0}, dL_m[2] = {0, 0};
+    for (size_t i = 0; i < qx.size(); ++i)
+        for (size_t j = 0; j < qx.size(); ++j) {
+            const double W = qw[i] * qw[j];
+            const double dx = px + qx[i] - p.m2[0], dy = py + qx[j] - p.m2[1];
+            const double G = std::exp(-0.5 * (p.conic[0] * dx * dx + p.conic[2] * dy * dy) - p.conic[1] * dx * dy);
+            const double oG = p.op * G;
+            Lp += W * -std::log1p(-oG);
+            const double w = W * oG / (1.0 - oG);
+            dL_op += w / p.op;
+            dL_c[0] += w * (-0.5 * dx * dx);
+            dL_c[1] += w * (-dx * dy);
+            dL_c[2] += w * (-0.5 * dy * dy);
+            dL_m[0] += w * (p.conic[0] * dx + p.conic[1] * dy);
+            dL_m[1] += w * (p.conic[1] * dx + p.conic[2] * dy);
+        }
+    double h, dh_dL, dh_dlam;
+    if (g.poisson) {
+        h = -std::expm1(-Lp);
+        dh_dL = std::exp(-Lp);
+        dh_dlam = 0.0;
+    } else {
+        const double Z = 1.0 - Lp / g.lam;
+        double Q = 0.0, dQ_dZ = 0.0, dQ_dlam = 0.0, Zn = 1.0;
+        for (size_t n = 0; n < g.law.P.size(); ++n) {
+            Q += g.law.P[n] * Zn;
+            dQ_dlam += g.law.dP[n] * Zn;
+            if (n + 1 < g.law.P.size()) dQ_dZ += (n + 1) * g.law.P[n + 1] * Zn;
+            Zn *= Z;
+        }
+        h = 1.0 - Q;
+        dh_dL = dQ_dZ / g.lam;
+        dh_dlam = -dQ_dZ * Lp / (g.lam * g.lam) - dQ_dlam;
+    }
+    FragP f;
+    f.p = h;
+    f.d_op = dh_dL * dL_op + dh_dlam * g.d_lam[0];
+    for (int c = 0; c < 3; ++c) f.d_conic[c] = dh_dL * dL_c[c] + dh_dlam * g.d_lam[1 + c];
+    f.d_m2[0] = dh_dL * dL_m[0];
+    f.d_m2[1] = dh_dL * dL_m[1];
+    return f;
+}
+
 }  // namespace
 
 extern "C" {
+
+// Law of the GPS point count at lambda (tests): writes up to `cap` probabilities P(N = n) and their
+// lambda-derivatives, returns how many the law has (may exceed cap).
+int oracle_gps_count_law(const double lambda, double* P, double* dP, const int cap) {
+    const CountLaw law = cf_count_law(lambda);
+    for (int n = 0; n < cap && n < static_cast<int>(law.P.size()); ++n) {
+        P[n] = law.P[n];
+        dP[n] = law.dP[n];
+    }
+    return static_cast<int>(law.P.size());
+}
 
 // Expected image (H, W, 3 / 1 / 1) of one stochastic-transparency sample, image resolution (the
 // ss x ss box filter applied), and the gradient of L = sum(g_image * image + g_alpha * alpha +
@@ -1052,7 +1290,34 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
                           const float* base_rotations, const float* base_opacities, const double* g_image,
                           const double* g_alpha, const double* g_depth, double* image, double* alpha, double* depth,
                           double* loss, double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
-                          double* d_sh) {
+                          double* d_sh);
+
+// The same for Gaussian point splatting: each fragment's alpha is replaced by the probability that
+// the Gaussian puts a point into the (sub)pixel (see gps_fragment), with the pixel integrals taken
+// by an order-`quad` Gauss-Legendre rule per axis. The support is the pixels whose centre passes the
+// power test at the base point, as in the render (scatter_utils.cuh:116-129).
+int oracle_expected_image_gps(const double* means, const double* scales, const double* rotations,
+                              const double* opacities, const double* sh, uint32_t n, uint32_t bases, const double* w2c,
+                              const double* cam_pos, uint32_t width, uint32_t height, double fx, double fy, double cx,
+                              double cy, double near_plane, double far_plane, int ss_raw, int aa,
+                              const float* base_means, const float* base_scales, const float* base_rotations,
+                              const float* base_opacities, const double* g_image, const double* g_alpha,
+                              const double* g_depth, double* image, double* alpha, double* depth, double* loss,
+                              double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
+                              double* d_sh, int quad);
+
+}  // extern "C"
+
+namespace {
+
+int expected_image_impl(const double* means, const double* scales, const double* rotations, const double* opacities,
+                        const double* sh, uint32_t n, uint32_t bases, const double* w2c, const double* cam_pos,
+                        uint32_t width, uint32_t height, double fx, double fy, double cx, double cy, double near_plane,
+                        double far_plane, int ss_raw, int aa, const float* base_means, const float* base_scales,
+                        const float* base_rotations, const float* base_opacities, const double* g_image,
+                        const double* g_alpha, const double* g_depth, double* image, double* alpha, double* depth,
+                        double* loss, double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
+                        double* d_sh, const bool gps, const int quad) {
     const uint32_t ss = ss_raw < 1 ? 1u : static_cast<uint32_t>(ss_raw);
     float w2cf[12];
     for (int i = 0; i < 12; ++i) w2cf[i] = static_cast<float>(w2c[i]);
@@ -1072,7 +1337,14 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
         for (uint32_t yy = 0; yy < rc.h; ++yy)
             for (uint32_t xx = 0; xx < rc.w; ++xx) {
                 const uint32_t px = rc.x0 + xx, py = rc.y0 + yy;
-                if (st_alpha(p, static_cast<float>(px), static_cast<float>(py), false) < kMinAlpha) continue;
+                if (gps) {
+                    const float dcx = static_cast<float>(px) + 0.5f - p.mx, dcy = static_cast<float>(py) + 0.5f - p.my;
+                    const float power =
+                        0.5f * (p.conic[0] * dcx * dcx + p.conic[2] * dcy * dcy) + p.conic[1] * dcx * dcy;
+                    if (power > p.power) continue;
+                } else if (st_alpha(p, static_cast<float>(px), static_cast<float>(py), false) < kMinAlpha) {
+                    continue;
+                }
                 frags[static_cast<size_t>(py) * fbw + px].push_back({key, g});
             }
     }
@@ -1081,6 +1353,10 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
         pd[g] = project_d(means + 3 * g, scales + 3 * g, rotations + 4 * g, opacities[g], sh + static_cast<size_t>(g) * bases * 3,
                           bases, w2c, cam_pos, dfx, dfy, dcx, dcy, static_cast<double>(fbw), static_cast<double>(fbh), dil,
                           aa != 0);
+    std::vector<GpsLaw> laws(gps ? n : 0);
+    for (uint32_t g = 0; g < n && gps; ++g) laws[g] = gps_law(pd[g]);
+    std::vector<double> qx, qw;
+    if (gps) gauss_legendre01(std::max(quad, 1), qx, qw);
     const bool grad = d_means != nullptr;
     std::vector<GradProj> gp(grad ? n : 0);
     for (auto& x : gp) x = GradProj{};
@@ -1090,7 +1366,8 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
     std::fill(alpha, alpha + n_px, 0.0);
     std::fill(depth, depth + n_px, 0.0);
     double L = 0.0;
-    std::vector<double> al, ci, suffix_c, suffix_z;
+    std::vector<double> al;
+    std::vector<FragP> fp;
     for (uint32_t py = 0; py < fbh; ++py)
         for (uint32_t px = 0; px < fbw; ++px) {
             auto& f = frags[static_cast<size_t>(py) * fbw + px];
@@ -1098,12 +1375,12 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
             const size_t ip = static_cast<size_t>(py / ss) * width + px / ss;
             const size_t m = f.size();
             al.assign(m, 0.0);
+            fp.resize(m);
             std::vector<double> T(m + 1, 1.0);
             for (size_t k = 0; k < m; ++k) {
-                const ProjD& p = pd[f[k].second];
-                const double dx = px - (p.m2[0] - 0.5), dy = py - (p.m2[1] - 0.5);
-                const double e = -0.5 * (p.conic[0] * dx * dx + p.conic[2] * dy * dy) - p.conic[1] * dx * dy;
-                al[k] = p.op * std::exp(std::min(e, 0.0));
+                const uint32_t g = f[k].second;
+                fp[k] = gps ? gps_fragment(pd[g], laws[g], px, py, qx, qw) : st_fragment(pd[g], px, py);
+                al[k] = fp[k].p;
                 T[k + 1] = T[k] * (1.0 - al[k]);
             }
             double Cc[3] = {0, 0, 0}, Aa = 0, Dd = 0;
@@ -1139,15 +1416,12 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
                 GradProj& G = gp[g];
                 for (int ch = 0; ch < 3; ++ch) G.color[ch] += gi[ch] * a * T[kk];
                 G.depth += gdp * a * T[kk];
-                // a = op * exp(e), e = -0.5 (cX dx^2 + cZ dy^2) - cY dx dy, dx = px - (m2x - 0.5)
-                const double dx = px - (p.m2[0] - 0.5), dy = py - (p.m2[1] - 0.5);
-                const double dAe = dA * a;
-                G.op += dA * (a / p.op);
-                G.conic[0] += dAe * (-0.5 * dx * dx);
-                G.conic[1] += dAe * (-dx * dy);
-                G.conic[2] += dAe * (-0.5 * dy * dy);
-                G.m2[0] += dAe * (p.conic[0] * dx + p.conic[1] * dy);
-                G.m2[1] += dAe * (p.conic[1] * dx + p.conic[2] * dy);
+                // the fragment's probability through its partial derivatives
+                const FragP& q = fp[kk];
+                G.op += dA * q.d_op;
+                for (int c = 0; c < 3; ++c) G.conic[c] += dA * q.d_conic[c];
+                G.m2[0] += dA * q.d_m2[0];
+                G.m2[1] += dA * q.d_m2[1];
             }
         }
     if (loss) *loss = L;
@@ -1156,6 +1430,39 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
         project_d_backward(pd[g], gp[g], sh + static_cast<size_t>(g) * bases * 3, bases, w2c, dfx, dfy, d_means + 3 * g,
                            d_scales + 3 * g, d_rotations + 4 * g, d_opacities + g, d_sh + static_cast<size_t>(g) * bases * 3);
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_expected_image(const double* means, const double* scales, const double* rotations, const double* opacities,
+                          const double* sh, uint32_t n, uint32_t bases, const double* w2c, const double* cam_pos,
+                          uint32_t width, uint32_t height, double fx, double fy, double cx, double cy, double near_plane,
+                          double far_plane, int ss_raw, int aa, const float* base_means, const float* base_scales,
+                          const float* base_rotations, const float* base_opacities, const double* g_image,
+                          const double* g_alpha, const double* g_depth, double* image, double* alpha, double* depth,
+                          double* loss, double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
+                          double* d_sh) {
+    return expected_image_impl(means, scales, rotations, opacities, sh, n, bases, w2c, cam_pos, width, height, fx, fy,
+                               cx, cy, near_plane, far_plane, ss_raw, aa, base_means, base_scales, base_rotations,
+                               base_opacities, g_image, g_alpha, g_depth, image, alpha, depth, loss, d_means, d_scales,
+                               d_rotations, d_opacities, d_sh, false, 0);
+}
+
+int oracle_expected_image_gps(const double* means, const double* scales, const double* rotations,
+                              const double* opacities, const double* sh, uint32_t n, uint32_t bases, const double* w2c,
+                              const double* cam_pos, uint32_t width, uint32_t height, double fx, double fy, double cx,
+                              double cy, double near_plane, double far_plane, int ss_raw, int aa,
+                              const float* base_means, const float* base_scales, const float* base_rotations,
+                              const float* base_opacities, const double* g_image, const double* g_alpha,
+                              const double* g_depth, double* image, double* alpha, double* depth, double* loss,
+                              double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
+                              double* d_sh, int quad) {
+    return expected_image_impl(means, scales, rotations, opacities, sh, n, bases, w2c, cam_pos, width, height, fx, fy,
+                               cx, cy, near_plane, far_plane, ss_raw, aa, base_means, base_scales, base_rotations,
+                               base_opacities, g_image, g_alpha, g_depth, image, alpha, depth, loss, d_means, d_scales,
+                               d_rotations, d_opacities, d_sh, true, quad);
 }
 
 }  // extern "C"

@@ -164,6 +164,8 @@ SIGNATURES = {
                                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                             ctypes.c_float, ctypes.c_int, ctypes.c_void_p,
                                                             ctypes.c_void_p, ctypes.c_void_p]),
+    "sgs_gps_count_law_size": (ctypes.c_size_t, []),
+    "sgs_gps_count_law": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgs_conv3x3_weights_size": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     "sgs_conv3x3": (ctypes.c_int, [ctypes.POINTER(Conv3x3Args), ctypes.c_void_p]),
     "sgs_conv3x3_wgrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,

@@ -1,12 +1,16 @@
 """Differentiable rendering: gradients of the progressively averaged image w.r.t. the Gaussians.
 
 `render_samples(means, scales, rotations, opacities, sh, settings, n_samples)` renders n_samples
-stochastic-transparency samples (Reset, then Static: their plain average, as Renderer.py's
-SAMPLES_PER_PIXEL loop produces it) and returns (image, depth, alpha) like `History`, with a
-backward pass to all five parameter tensors (the reference renders only; it has no backward).
+samples (Reset, then Static: their plain average, as Renderer.py's SAMPLES_PER_PIXEL loop produces
+it) with stochastic transparency or Gaussian point splatting (`settings.use_gps`, scatter or hybrid
+scheduling) and returns (image, depth, alpha) like `History`, with a backward pass to all five
+parameter tensors (the reference renders only; it has no backward).
 
 The backward is an unbiased estimator of the gradient of the expected image (see
 csrc/backward_st.cu): each sample's winners give a one-sample estimate, averaged over the samples.
+For GPS a fragment's alpha is replaced by the probability that the Gaussian puts a point into the
+(sub)pixel, from the law of the point count the render draws and a quadrature of the point density
+over the pixel.
 The forward renders all samples in one call (`_C.render_samples`: one fragment walk, the samples'
 winner framebuffers side by side in its workspace, outputs bit-identical to one call per sample).
 Winners are either kept from the forward pass (`store_winners=True`, 8 bytes per framebuffer pixel
@@ -69,8 +73,8 @@ def _render_all(tensors, settings: Settings, n_samples: int, first_frame: int):
 class _RenderSamples(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means, scales, rotations, opacities, sh, settings, n_samples, first_frame, store_winners):
-        if settings.use_gps or settings.spatial_reuse:
-            raise RuntimeError("render_samples differentiates stochastic transparency without spatial reuse")
+        if settings.spatial_reuse:
+            raise RuntimeError("render_samples does not differentiate spatial reuse")
         tensors = tuple(t.detach().contiguous() for t in (means, scales, rotations, opacities, sh))
         (image, depth, alpha, _), ws, layout = _render_all(tensors, settings, n_samples, first_frame)
         ctx.save_for_backward(*tensors)
@@ -120,8 +124,9 @@ class _RenderSamples(torch.autograd.Function):
 
 def render_samples(means, scales, rotations, opacities, sh_coefficients, settings: Settings, n_samples: int = 1,
                    first_frame: int | None = None, store_winners: bool = True):
-    """Differentiable average of `n_samples` stochastic-transparency samples: (image, depth, alpha),
-    premultiplied by alpha like `History`. Frames first_frame .. first_frame + n_samples - 1 (default:
+    """Differentiable average of `n_samples` samples (stochastic transparency or, with
+    `settings.use_gps`, Gaussian point splatting): (image, depth, alpha), premultiplied by alpha like
+    `History`. Frames first_frame .. first_frame + n_samples - 1 (default:
     the process-wide frame index, which advances by n_samples)."""
     if first_frame is None:
         first_frame = _C.get_frame_index()

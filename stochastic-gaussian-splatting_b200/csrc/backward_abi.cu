@@ -14,13 +14,13 @@ constexpr size_t kAccumFloats = 10;
 struct BackwardSetup {
     BackwardParams p;
     sgs_workspace_layout layout;
+    bool gps;
 };
 
 int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, BackwardSetup& out) {
     if (g == nullptr || c == nullptr || s == nullptr) return record_error(SGS_ERROR_INVALID_ARGUMENT, "null argument");
-    if (s->use_gps || s->spatial_reuse)
-        return record_error(SGS_ERROR_INVALID_ARGUMENT,
-                            "the backward pass supports stochastic transparency without spatial reuse");
+    if (s->spatial_reuse)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT, "the backward pass does not support spatial reuse");
     if (g->sh_bases != 1 && g->sh_bases != 4 && g->sh_bases != 9 && g->sh_bases != 16)
         return record_error(SGS_ERROR_INVALID_ARGUMENT, "sh_bases must be 1, 4, 9 or 16");
     if (g->quantized != nullptr)
@@ -58,6 +58,8 @@ int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, Ba
     p.width = c->width;
     p.ss = ss;
     p.n_fb = c->width * ss * c->height * ss;
+    p.gps_law = nullptr;
+    out.gps = s->use_gps != 0;
     return SGS_OK;
 }
 
@@ -65,19 +67,22 @@ constexpr uint32_t kMaxFusedSamples = 1024;
 
 size_t align256(const size_t v) { return (v + 255) & ~size_t(255); }
 
-// Interleaved per-pixel sample table of the fused backward: keys, then terms.
-void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples) {
+// Interleaved per-pixel sample table of the fused backward: keys, then terms, the per-pixel largest
+// key, and for GPS the count-law table.
+void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples, const bool gps) {
     p.n_samples = n_samples;
     p.pix_keys = static_cast<unsigned long long*>(scratch);
     const size_t keys = align256(sizeof(unsigned long long) * p.n_fb * static_cast<size_t>(n_samples));
     const size_t terms = align256(sizeof(float) * p.n_fb * static_cast<size_t>(n_samples));
+    const size_t max_keys = align256(sizeof(unsigned long long) * p.n_fb);
     p.pix_terms = reinterpret_cast<float*>(static_cast<char*>(scratch) + keys);
     p.pix_max_key = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + keys + terms);
+    p.gps_law = gps ? reinterpret_cast<float2*>(static_cast<char*>(scratch) + keys + terms + max_keys) : nullptr;
 }
 
 // Entries of the large-Gaussian queue of the fused walk (at most 2^18).
 uint32_t queue_capacity(const uint32_t n) { return n < (1u << 18) ? n : (1u << 18); }
-constexpr size_t kWalkGaussianBytes = 96;
+constexpr size_t kWalkGaussianBytes = 128;  // walk constants (96) and GPS constants (32)
 
 // Backward workspace: colours (3 per Gaussian, padded to 4), accumulators (10 per Gaussian), then
 // the fused walk's queue (header, entries, meta, indices), each section 256-byte aligned.
@@ -123,6 +128,10 @@ int sgs_backward_accumulate(const sgs_gaussians* gaussians, const sgs_camera* ca
     BackwardSetup S;
     int st = setup(gaussians, camera, settings, S);
     if (st != SGS_OK) return st;
+    if (S.gps)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT,
+                            "GPS gradients use the fused walk (sgs_backward_accumulate_samples or "
+                            "sgs_backward_accumulate_framebuffers)");
     if (render_workspace == nullptr || grad_image == nullptr || backward_workspace == nullptr ||
         (reinterpret_cast<uintptr_t>(backward_workspace) & 15u) != 0)
         return record_error(SGS_ERROR_INVALID_ARGUMENT, "null render workspace, image gradient or backward workspace");
@@ -152,7 +161,17 @@ size_t sgs_backward_samples_scratch_size(const sgs_camera* camera, const sgs_set
     const uint32_t ss = settings->supersampling_factor < 1 ? 1u : static_cast<uint32_t>(settings->supersampling_factor);
     const size_t n_fb = static_cast<size_t>(camera->width) * ss * camera->height * ss;
     return align256(sizeof(unsigned long long) * n_fb * n_samples) + align256(sizeof(float) * n_fb * n_samples) +
-           align256(sizeof(unsigned long long) * n_fb);
+           align256(sizeof(unsigned long long) * n_fb) + (settings->use_gps ? align256(gps_count_law_bytes()) : 0);
+}
+
+size_t sgs_gps_count_law_size(void) { return gps_count_law_bytes(); }
+
+int sgs_gps_count_law(void* out, void* stream_ptr) {
+    if (out == nullptr || (reinterpret_cast<uintptr_t>(out) & 7u) != 0)
+        return record_error(SGS_ERROR_INVALID_ARGUMENT, "the count-law table needs an 8-byte aligned device buffer");
+    const cudaError_t err = launch_gps_count_law(static_cast<float2*>(out), static_cast<cudaStream_t>(stream_ptr));
+    if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "count law: %s", cudaGetErrorString(err));
+    return SGS_OK;
 }
 
 int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* camera, const sgs_settings* settings,
@@ -177,7 +196,7 @@ int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* 
     p.grad_alpha = grad_alpha;
     p.grad_depth = grad_depth;
     p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
-    set_sample_table(p, scratch, n_samples);
+    set_sample_table(p, scratch, n_samples, S.gps);
     p.sample = sample;
     const cudaError_t err = launch_backward_sample_terms(p, static_cast<cudaStream_t>(stream_ptr));
     if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
@@ -203,7 +222,7 @@ int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_ca
     p.grad_alpha = grad_alpha;
     p.grad_depth = grad_depth;
     p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
-    set_sample_table(p, scratch, n_samples);
+    set_sample_table(p, scratch, n_samples, S.gps);
     set_backward_buffers(p, backward_workspace);
     cudaError_t err = cudaSuccess;
     if (first) {
@@ -243,7 +262,7 @@ int sgs_backward_accumulate_framebuffers(const sgs_gaussians* gaussians, const s
     p.grad_alpha = grad_alpha;
     p.grad_depth = grad_depth;
     p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
-    set_sample_table(p, scratch, n_samples);
+    set_sample_table(p, scratch, n_samples, S.gps);
     set_backward_buffers(p, backward_workspace);
     cudaError_t err = cudaSuccess;
     if (first) err = cudaMemsetAsync(p.accum, 0, kAccumFloats * p.n * sizeof(float), stream);

@@ -32,6 +32,224 @@ constexpr uint32_t kChunkPixels = 2048;   // pixels per stolen chunk (whole rows
 constexpr uint32_t kQueueBlocksPerSM = 8;
 constexpr int kAccum = 10;               // op, conic x/y/z, mean2d x/y, depth, colour r/g/b
 
+// ---- Gaussian point splatting: the probability that a Gaussian puts a point into a pixel ----------
+// A GPS Gaussian (projected opacity o, dilated 2-D covariance with conic C, mean m) draws
+// N = rint(max(kf(w), 0)) points, w standard normal and kf the Cornish-Fisher expansion of a Poisson
+// quantile at lambda = 2 pi sqrt(det) Li2(o) (math_utils.h:98-111, accumulate_scatter.cu:104-112),
+// each independently with density -ln(1 - o G(x)) / lambda, G(x) = exp(-(x - m)^T C (x - m) / 2)
+// (truncated_box_muller). A point in the square of a (sub)pixel whose centre passes the power test
+// registers there, so the Gaussian reaches the pixel with probability h = 1 - Q,
+//   Q = E[(1 - q)^N] = sum_n P(N = n) (1 - q)^n,  q = Lambda_p / lambda,
+//   Lambda_p = integral over the pixel square of -ln(1 - o G),
+// independently of the other Gaussians: the stochastic-transparency estimator holds with alpha
+// replaced by h. Lambda_p and its derivatives come from a 3 x 3 Gauss-Legendre rule over the pixel.
+// P(N = n) and dP/dlambda come from a table over log2(lambda) in [-10, 3] (32 terms, the rest of
+// the law folded into the last), built per call by gps_count_law_kernel; from lambda = 8 up the
+// count is taken as Poisson (Q = exp(-Lambda_p)), which the draw matches there to within 3e-4.
+constexpr int kLawRows = 1025;
+constexpr int kLawTerms = 32;
+constexpr float kLawLog2Min = -10.0f;
+constexpr float kLawLog2Span = 13.0f;
+static_assert(kLawTerms == 32, "one lane of the table kernel per term");
+
+// kf(w) at lambda and its partial derivatives in w and lambda
+__device__ __forceinline__ double law_kf(const double w, const double lam) {
+    const double s = sqrt(lam), w2 = w * w;
+    return lam + s * w + (w2 - 1.0) / 6.0 + (-(w / 36.0) - w2 * w / 72.0) / s +
+           (-(8.0 / 405.0) + (7.0 / 810.0) * w2 + w2 * w2 / 270.0) / lam;
+}
+__device__ __forceinline__ double law_kf_w(const double w, const double lam) {
+    const double s = sqrt(lam), w2 = w * w;
+    return s + w / 3.0 + (-(1.0 / 36.0) - w2 / 24.0) / s + ((14.0 / 810.0) * w + (4.0 / 270.0) * w2 * w) / lam;
+}
+__device__ __forceinline__ double law_kf_lam(const double w, const double lam) {
+    const double s = sqrt(lam), w2 = w * w;
+    return 1.0 + w / (2.0 * s) - 0.5 * (-(w / 36.0) - w2 * w / 72.0) / (lam * s) -
+           (-(8.0 / 405.0) + (7.0 / 810.0) * w2 + w2 * w2 / 270.0) / (lam * lam);
+}
+
+// One warp per table row (lambda = 2^(kLawLog2Min + kLawLog2Span r / (kLawRows - 1))). The quartic kf
+// is monotone between the roots of kf' on [-12, 12] (outside, kf exceeds every threshold used); lane n
+// computes F(n + 1/2) = P(kf(w) < n + 1/2) over those pieces and its lambda-derivative
+// -sum over the roots r of kf = t of phi(r) (dkf/dlambda)(r) / |dkf/dw(r)|; then P(N = n) =
+// F(n + 1/2) - F(n - 1/2), and the last term takes all of N >= kLawTerms - 1. Stored as (P, dP).
+__global__ void __launch_bounds__(32) gps_count_law_kernel(float2* __restrict__ law) {
+    constexpr double kW = 12.0;
+    constexpr int kPerLane = 150;  // 32 x 150 grid intervals of kf' over [-kW, kW]
+    constexpr int kMaxCuts = 16;
+    __shared__ double s_cut[kMaxCuts + 2];
+    __shared__ int s_n;
+    const uint32_t lane = threadIdx.x;
+    const double lam = exp2(static_cast<double>(kLawLog2Min) +
+                            static_cast<double>(kLawLog2Span) * blockIdx.x / static_cast<double>(kLawRows - 1));
+    if (lane == 0) s_n = 0;
+    __syncwarp();
+    const double step = 2.0 * kW / (32.0 * kPerLane);
+    double w_prev = -kW + step * kPerLane * lane;
+    double d_prev = law_kf_w(w_prev, lam);
+    for (int i = 1; i <= kPerLane; ++i) {
+        const double w = -kW + step * (kPerLane * lane + i);
+        const double d = law_kf_w(w, lam);
+        if ((d_prev < 0.0) != (d < 0.0)) {
+            double lo = w_prev, hi = w;
+            const bool lo_neg = d_prev < 0.0;
+            for (int it = 0; it < 64 && hi - lo > 1e-15; ++it) {
+                const double mid = 0.5 * (lo + hi);
+                if ((law_kf_w(mid, lam) < 0.0) == lo_neg) lo = mid;
+                else hi = mid;
+            }
+            const int slot = atomicAdd(&s_n, 1);
+            if (slot < kMaxCuts) s_cut[slot + 1] = 0.5 * (lo + hi);
+        }
+        w_prev = w;
+        d_prev = d;
+    }
+    __syncwarp();
+    const int n_cut = min(s_n, kMaxCuts);
+    if (lane == 0) {
+        // insertion sort of the interior cuts, framed by the ends of the interval
+        for (int i = 2; i <= n_cut; ++i) {
+            const double v = s_cut[i];
+            int j = i - 1;
+            while (j >= 1 && s_cut[j] > v) {
+                s_cut[j + 1] = s_cut[j];
+                --j;
+            }
+            s_cut[j + 1] = v;
+        }
+        s_cut[0] = -kW;
+        s_cut[n_cut + 1] = kW;
+    }
+    __syncwarp();
+    const double t = lane + 0.5;
+    double F = 0.0, dF = 0.0;
+    for (int i = 0; i <= n_cut; ++i) {
+        const double a = s_cut[i], bnd = s_cut[i + 1];
+        const double fa = law_kf(a, lam), fb = law_kf(bnd, lam);
+        const bool up = fb >= fa;
+        const double lo_v = up ? fa : fb, hi_v = up ? fb : fa;
+        if (t <= lo_v) continue;
+        const double ca = 0.5 * erfc(-a * 0.70710678118654752), cb = 0.5 * erfc(-bnd * 0.70710678118654752);
+        if (t >= hi_v) {
+            F += cb - ca;
+            continue;
+        }
+        double lo = a, hi = bnd;
+        for (int it = 0; it < 64 && hi - lo > 1e-15; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if ((law_kf(mid, lam) < t) == up) lo = mid;
+            else hi = mid;
+        }
+        const double r = 0.5 * (lo + hi);
+        const double cr = 0.5 * erfc(-r * 0.70710678118654752);
+        F += up ? cr - ca : cb - cr;
+        const double slope = fabs(law_kf_w(r, lam));
+        if (slope > 0.0) dF -= exp(-0.5 * r * r) * 0.39894228040143268 * law_kf_lam(r, lam) / slope;
+    }
+    double F_below = __shfl_up_sync(0xffffffffu, F, 1);
+    double dF_below = __shfl_up_sync(0xffffffffu, dF, 1);
+    if (lane == 0) {
+        F_below = 0.0;
+        dF_below = 0.0;
+    }
+    double P = F - F_below, dP = dF - dF_below;
+    if (lane == kLawTerms - 1) {  // N >= kLawTerms - 1
+        P = 1.0 - F_below;
+        dP = -dF_below;
+    }
+    law[static_cast<size_t>(blockIdx.x) * kLawTerms + lane] = make_float2(static_cast<float>(P), static_cast<float>(dP));
+}
+
+// Per-Gaussian constants of the GPS hit probability.
+struct GpsConstants {
+    float lambda;      // expected point count
+    float d_lambda[4]; // d lambda / d (opacity, conic x, y, z)
+    float law_pos;     // row position of lambda in the count table; kLawRows - 1: Poisson
+    float pad[2];
+};
+
+__device__ __forceinline__ GpsConstants gps_constants(const Projected& p) {
+    GpsConstants c;
+    const float sd = sqrtf(p.determinant);
+    const float lam = kTwoPi * sd * gps_dilog(p.opacity);
+    const float D = p.conic.x * p.conic.z - p.conic.y * p.conic.y;  // 1 / det
+    c.lambda = lam;
+    c.d_lambda[0] = kTwoPi * sd * (-logf(fmaxf(1.0f - p.opacity, 1.0e-7f)) / p.opacity);  // Li2'(o) = -ln(1 - o) / o
+    c.d_lambda[1] = -0.5f * lam * p.conic.z / D;
+    c.d_lambda[2] = lam * p.conic.y / D;
+    c.d_lambda[3] = -0.5f * lam * p.conic.x / D;
+    const float pos = (log2f(lam) - kLawLog2Min) * (static_cast<float>(kLawRows - 1) / kLawLog2Span);
+    c.law_pos = fminf(fmaxf(pos, 0.0f), static_cast<float>(kLawRows - 1));
+    c.pad[0] = c.pad[1] = 0.0f;
+    return c;
+}
+
+// Q (no point of the Gaussian in the pixel) and its derivatives in the projected opacity, the conic
+// and the 2-D mean, for the pixel whose centre lies at (dx0, dy0) from the mean.
+struct GpsFragment {
+    float Q, dQ_op, dQ_conic[3], dQ_m[2];
+};
+
+__device__ __forceinline__ GpsFragment gps_fragment(const float cx, const float cy, const float cz, const float op,
+                                                    const float3 conic, const GpsConstants& c, const float dx0,
+                                                    const float dy0, const float2* __restrict__ law) {
+    constexpr float kOff = 0.38729833462074170f;  // Gauss-Legendre nodes of [0, 1]: 1/2 +- sqrt(3/5) / 2
+    constexpr float kWe = 5.0f / 18.0f, kWm = 8.0f / 18.0f;
+    float L = 0.0f, s_o = 0.0f, s_xx = 0.0f, s_xy = 0.0f, s_yy = 0.0f, s_x = 0.0f, s_y = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float dx = dx0 + static_cast<float>(i - 1) * kOff;
+        const float wi = i == 1 ? kWm : kWe;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float dy = dy0 + static_cast<float>(j - 1) * kOff;
+            const float W = wi * (j == 1 ? kWm : kWe);
+            const float e = dx * (cx * dx + cy * dy) + cz * dy * dy;  // log2 G
+            const float oG = op * exp2f(fminf(e, 0.0f));
+            const float rest = 1.0f - oG;
+            L -= W * logf(rest);
+            const float w = W * oG / rest;
+            s_o += w;
+            s_xx += w * dx * dx;
+            s_xy += w * dx * dy;
+            s_yy += w * dy * dy;
+            s_x += w * dx;
+            s_y += w * dy;
+        }
+    }
+    float Q, dQ_dL, dQ_dlam;
+    if (c.law_pos >= static_cast<float>(kLawRows - 1)) {
+        Q = expf(-L);
+        dQ_dL = -Q;
+        dQ_dlam = 0.0f;
+    } else {
+        const int row = static_cast<int>(c.law_pos);
+        const float t = c.law_pos - static_cast<float>(row);
+        const float2* r0 = law + static_cast<size_t>(row) * kLawTerms;
+        const float2* r1 = r0 + kLawTerms;
+        const float Z = fmaxf(1.0f - L / c.lambda, 0.0f);
+        float dZ = 0.0f, dl = 0.0f;
+        Q = 0.0f;
+        for (int n = kLawTerms - 1; n >= 0; --n) {
+            const float2 a = r0[n], b = r1[n];
+            dZ = dZ * Z + Q;
+            Q = Q * Z + (a.x + t * (b.x - a.x));
+            dl = dl * Z + (a.y + t * (b.y - a.y));
+        }
+        dQ_dL = -dZ / c.lambda;
+        dQ_dlam = dZ * L / (c.lambda * c.lambda) + dl;
+    }
+    GpsFragment f;
+    f.Q = Q;
+    f.dQ_op = dQ_dL * (s_o / op) + dQ_dlam * c.d_lambda[0];
+    f.dQ_conic[0] = dQ_dL * (-0.5f * s_xx) + dQ_dlam * c.d_lambda[1];
+    f.dQ_conic[1] = dQ_dL * (-s_xy) + dQ_dlam * c.d_lambda[2];
+    f.dQ_conic[2] = dQ_dL * (-0.5f * s_yy) + dQ_dlam * c.d_lambda[3];
+    f.dQ_m[0] = dQ_dL * (conic.x * s_x + conic.y * s_y);
+    f.dQ_m[1] = dQ_dL * (conic.y * s_x + conic.z * s_y);
+    return f;
+}
+
 // View-dependent colour of every Gaussian (the colour its fragments would give a pixel).
 __global__ void __launch_bounds__(kBlock) colors_kernel(const BackwardParams b) {
     const uint32_t g = blockIdx.x * kBlock + threadIdx.x;
@@ -223,13 +441,23 @@ struct WalkGaussian {
     uint32_t row_first;       // first row position in the warp's row list
     uint32_t pad[2];
 };
-static_assert(sizeof(WalkGaussian) == 96, "the backward workspace reserves 96 bytes per queue entry");
+static_assert(sizeof(WalkGaussian) == 96, "WalkEntry pairs it with 32 bytes of GPS constants");
 
+
+// A queue entry of the fused walk: the walk constants and, for GPS, the hit-probability constants.
+struct WalkEntry {
+    WalkGaussian g;
+    GpsConstants c;
+};
+static_assert(sizeof(WalkEntry) == 128, "the backward workspace reserves 128 bytes per queue entry");
 
 // Lane walks the span of row y of Gaussian q (when valid), one pixel per step, and adds the S
-// samples' fragment gradients to acc.
-__device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, const WalkGaussian& q, const bool valid,
-                                                   const uint32_t y, FragAccum& acc, const uint32_t seg = 0,
+// samples' fragment gradients to acc. kGps: the fragment probability is the GPS hit probability
+// (constants gc) instead of alpha.
+template <bool kGps>
+__device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, const WalkGaussian& q,
+                                                   const GpsConstants& gc, const bool valid, const uint32_t y,
+                                                   FragAccum& acc, const uint32_t seg = 0,
                                                    const uint32_t log_segs = 0) {
     uint32_t xs = 0, len = 0;
     float dy = 0.0f;
@@ -287,9 +515,7 @@ __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, cons
                     none += kk == kEmptyFragment;
                     if (kk > key_k) behind += terms[s];
                 }
-                const float inv = 1.0f / fmaxf(1.0f - alpha, 1e-12f);
                 const float gck = g0 * q.ckx + g1 * q.cky + g2 * q.ckz + gd * q.depth;
-                const float dA = static_cast<float>(ge) * gck - inv * behind + inv * ga * static_cast<float>(none);
                 if (won != 0) {
                     const float wf = static_cast<float>(won);
                     acc.v[6] += gd * wf;
@@ -297,14 +523,31 @@ __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, cons
                     acc.v[8] += g1 * wf;
                     acc.v[9] += g2 * wf;
                 }
-                // alpha = opacity exp(-0.5 (cX dx^2 + cZ dy^2) - cY dx dy)
-                const float dAe = dA * alpha;
-                acc.v[0] += dA * (alpha / q.opacity);
-                acc.v[1] += dAe * (-0.5f * dx * dx);
-                acc.v[2] += dAe * (-dx * dy);
-                acc.v[3] += dAe * (-0.5f * dy * dy);
-                acc.v[4] += dAe * (q.conic_x * dx + q.conic_y * dy);
-                acc.v[5] += dAe * (q.conic_y * dx + q.conic_z * dy);
+                if (kGps) {
+                    // h = 1 - Q: dL/dh from the samples, then through Q's partial derivatives
+                    const GpsFragment f = gps_fragment(q.cx, q.cy, q.cz, q.opacity,
+                                                       make_float3(q.conic_x, q.conic_y, q.conic_z), gc, dx, dy,
+                                                       b.gps_law);
+                    const float inv = 1.0f / fmaxf(f.Q, 1e-12f);
+                    const float dH = static_cast<float>(ge) * gck - inv * behind + inv * ga * static_cast<float>(none);
+                    acc.v[0] -= dH * f.dQ_op;
+                    acc.v[1] -= dH * f.dQ_conic[0];
+                    acc.v[2] -= dH * f.dQ_conic[1];
+                    acc.v[3] -= dH * f.dQ_conic[2];
+                    acc.v[4] -= dH * f.dQ_m[0];
+                    acc.v[5] -= dH * f.dQ_m[1];
+                } else {
+                    const float inv = 1.0f / fmaxf(1.0f - alpha, 1e-12f);
+                    const float dA = static_cast<float>(ge) * gck - inv * behind + inv * ga * static_cast<float>(none);
+                    // alpha = opacity exp(-0.5 (cX dx^2 + cZ dy^2) - cY dx dy)
+                    const float dAe = dA * alpha;
+                    acc.v[0] += dA * (alpha / q.opacity);
+                    acc.v[1] += dAe * (-0.5f * dx * dx);
+                    acc.v[2] += dAe * (-dx * dy);
+                    acc.v[3] += dAe * (-0.5f * dy * dy);
+                    acc.v[4] += dAe * (q.conic_x * dx + q.conic_y * dy);
+                    acc.v[5] += dAe * (q.conic_y * dx + q.conic_z * dy);
+                }
             }
         }
         fx += 1.0f;
@@ -317,8 +560,10 @@ __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, cons
 
 // One thread per Gaussian: the rows of a warp's 32 Gaussians are laid end to end, 32 per step, and
 // each lane walks one row; the row sums go to per-Gaussian accumulators in shared memory.
+template <bool kGps>
 __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const BackwardParams b) {
     __shared__ WalkGaussian s_g[kWarpsPerBlock][32];
+    __shared__ GpsConstants s_c[kGps ? kWarpsPerBlock : 1][32];
     __shared__ float s_acc[kWarpsPerBlock][32][kAccum];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t wib = threadIdx.x >> 5;
@@ -334,6 +579,8 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
     const PixelRect rect = pixel_rect(p.bounds, b.cam);
     bool has_rows = active && rect.width > 0 && rect.height > 0;
     WalkGaussian q;
+    GpsConstants c{};
+    if (kGps && has_rows) c = gps_constants(p);
     if (has_rows) {
         q.mx = p.mean2d.x - 0.5f;
         q.my = p.mean2d.y - 0.5f;
@@ -365,7 +612,9 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
             const uint32_t e = static_cast<uint32_t>(old >> kQueueEntryShift);
             const unsigned long long first_chunk = old & kQueueChunkMask;
             if (e < b.bw_capacity && first_chunk + chunks <= kMaxQueueChunks) {
-                static_cast<WalkGaussian*>(b.bw_entries)[e] = q;
+                WalkEntry* entry = static_cast<WalkEntry*>(b.bw_entries) + e;
+                entry->g = q;
+                if (kGps) entry->c = c;
                 b.bw_meta[e] = make_uint4(rect.y_min, rect.height, log_rpc, static_cast<uint32_t>(first_chunk));
                 b.bw_index[e] = g;
                 has_rows = false;
@@ -383,6 +632,7 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
     if (has_rows) {
         q.row_first = row_incl - h;
         s_g[wib][slot] = q;
+        if (kGps) s_c[wib][slot] = c;
     }
     __syncwarp();
     int prev = -1;
@@ -394,10 +644,11 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
         const uint32_t r = base + lane;
         const bool valid = r < total_rows;
         const WalkGaussian rq = s_g[wib][valid ? owner : 0];
+        const GpsConstants rc = kGps ? s_c[wib][valid ? owner : 0] : GpsConstants{};
         FragAccum acc;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
-        walk_row_gradients(b, rq, valid, rq.y_min + (r - rq.row_first), acc);
+        walk_row_gradients<kGps>(b, rq, rc, valid, rq.y_min + (r - rq.row_first), acc);
         if (valid) {
 #pragma unroll
             for (int i = 0; i < kAccum; ++i)
@@ -417,6 +668,7 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
 // Persistent consumer of the fused walk's large-Gaussian queue: each warp steals one chunk of rows
 // (R rows, each split into 32 / R lane segments), sums the lanes' gradients and adds them to the
 // Gaussian's accumulators.
+template <bool kGps>
 __global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const BackwardParams b) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long packed = b.bw_queue->packed;
@@ -428,7 +680,7 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const B
         last_entry = queue_entry_of_chunk(b.bw_meta, n_entries, kUnusedQueueEntry - 1u, lane);
     const uint4 last = b.bw_meta[last_entry];
     const uint32_t n_chunks = last.w + ((last.y + (1u << last.z) - 1u) >> last.z);
-    const WalkGaussian* entries = static_cast<const WalkGaussian*>(b.bw_entries);
+    const WalkEntry* entries = static_cast<const WalkEntry*>(b.bw_entries);
     for (;;) {
         uint32_t c = 0;
         if (lane == 0) c = atomicAdd(&b.bw_queue->next_chunk, 1u);
@@ -447,12 +699,13 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const B
             if (lane == 0) atomicOr(&b.bw_queue->error, 1u);
             continue;
         }
-        const WalkGaussian q = entries[lo];
+        const WalkGaussian q = entries[lo].g;
+        const GpsConstants gc = kGps ? entries[lo].c : GpsConstants{};
         const uint32_t r = r0 + (lane & ((1u << log_rows) - 1u));
         FragAccum acc;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
-        walk_row_gradients(b, q, r < m.y, q.y_min + r, acc, lane >> log_rows, 5u - log_rows);
+        walk_row_gradients<kGps>(b, q, gc, r < m.y, q.y_min + r, acc, lane >> log_rows, 5u - log_rows);
         float* out = b.accum + static_cast<size_t>(b.bw_index[lo]) * kAccum;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) {
@@ -673,8 +926,23 @@ cudaError_t launch_backward_sample_terms(const BackwardParams& p, cudaStream_t s
 
 cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStream_t stream) {
     if (p.n == 0) return cudaSuccess;
-    fragments_samples_kernel<<<(p.n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(p);
-    fragments_samples_queue_kernel<<<static_cast<unsigned>(max(p.num_sms, 1)) * kQueueBlocksPerSM, kBlock, 0, stream>>>(p);
+    const unsigned grid = (p.n + kBlock - 1) / kBlock;
+    const unsigned queue_grid = static_cast<unsigned>(max(p.num_sms, 1)) * kQueueBlocksPerSM;
+    if (p.gps_law != nullptr) {
+        gps_count_law_kernel<<<kLawRows, 32, 0, stream>>>(p.gps_law);
+        fragments_samples_kernel<true><<<grid, kBlock, 0, stream>>>(p);
+        fragments_samples_queue_kernel<true><<<queue_grid, kBlock, 0, stream>>>(p);
+    } else {
+        fragments_samples_kernel<false><<<grid, kBlock, 0, stream>>>(p);
+        fragments_samples_queue_kernel<false><<<queue_grid, kBlock, 0, stream>>>(p);
+    }
+    return cudaGetLastError();
+}
+
+size_t gps_count_law_bytes() { return sizeof(float2) * static_cast<size_t>(kLawRows) * kLawTerms; }
+
+cudaError_t launch_gps_count_law(float2* law, cudaStream_t stream) {
+    gps_count_law_kernel<<<kLawRows, 32, 0, stream>>>(law);
     return cudaGetLastError();
 }
 

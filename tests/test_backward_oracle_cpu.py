@@ -9,8 +9,8 @@ from oracle import cpu
 KEYS = ("means", "scales", "rotations", "opacities", "sh_coefficients")
 
 
-def _setup(ss=1):
-    spec = sgs_scenes.SceneSpec(n=120, log_scale_mean=-2.3, log_scale_std=0.4, opacity_logit_std=1.0)
+def _setup(ss=1, n=120):
+    spec = sgs_scenes.SceneSpec(n=n, log_scale_mean=-2.3, log_scale_std=0.4, opacity_logit_std=1.0)
     scene = {k: t.numpy() for k, t in zip(KEYS, sgs_scenes.make_scene(spec, seed=5, morton=False).tensors())}
     cam = sgs_scenes.pinhole((0.3, -0.2, -4.0), 48, 36, 60.0)
     cd = dict(width=48, height=36, focal_x=cam.focal_x, focal_y=cam.focal_y, center_x=cam.center_x,
@@ -75,4 +75,106 @@ def test_analytic_gradient_matches_central_differences(aa):
             checked += 1
     worst.sort(reverse=True)
     assert checked >= 64
+    assert worst[0][0] < 2e-3, worst[:5]
+
+
+@pytest.mark.parametrize("aa,ss", [(False, 1), (True, 2)])
+def test_gps_expected_image_matches_the_monte_carlo_mean_of_the_oracle(aa, ss):
+    """Gaussian point splatting: the average of many samples of the oracle's GPS render (the
+    reference's point sampler restated, pinned to its golden outputs) converges to the expected image
+    built from the law of the point count and the point density integrated over each pixel. The mean
+    alpha error has no sign (the stochastic-transparency alpha at the pixel centre, the nearest wrong
+    model, is off by +0.0018 on this scene without antialiasing). 128 Gaussians: no partial warp (see
+    the next test)."""
+    scene, cd, *_ = _setup(n=128)
+    exp = cpu.expected_image(scene, cd, ss=ss, aa=aa, gps=True, quad=8)
+    flags = dict(aa=aa, ss=ss, gps=True, hybrid=False)
+    image = np.zeros((36, 48, 3))
+    alpha = np.zeros((36, 48, 1))
+    n = 1200
+    for f in range(n):
+        out = cpu.sample_resolve(scene, cd, flags, cpu.accumulate(scene, cd, flags, f, threads=2), threads=2)
+        image += out["image"]
+        alpha += out["alpha"]
+    err = np.abs(image / n - exp["image"])
+    bias = float((alpha / n - exp["alpha"]).mean())
+    assert float(exp["alpha"].mean()) > 0.05
+    assert err.mean() < 0.006 and np.percentile(err, 99) < 0.05, (err.mean(), np.percentile(err, 99))
+    assert abs(bias) < 0.0008, bias
+
+
+def test_gps_count_law_is_the_law_of_the_render_draw():
+    """The count law (roots of the Cornish-Fisher quartic) against the draw itself, in double precision
+    over 2M normal deviates, and its lambda-derivative against central differences."""
+    rng = np.random.default_rng(3)
+    w = rng.standard_normal(2_000_000)
+    for lam in (0.02, 0.1, 0.3, 1.0, 3.0, 12.0):
+        P, dP = cpu.gps_count_law(lam)
+        assert abs(P.sum() - 1.0) < 1e-12
+        s, w2 = np.sqrt(lam), w * w
+        kf = lam + s * w + (w2 - 1) / 6 + (-(w / 36) - w2 * w / 72) / s + (-(8 / 405) + (7 / 810) * w2 + w2 * w2 / 270) / lam
+        mc = np.bincount(np.rint(np.maximum(kf, 0)).astype(int), minlength=len(P))[:len(P)] / len(w)
+        se = np.sqrt(np.maximum(P * (1 - P), 1e-12) / len(w))
+        assert np.all(np.abs(mc - P) < 6 * se + 1e-6), lam
+        h = 1e-5 * lam
+        Pp, _ = cpu.gps_count_law(lam + h)
+        Pm, _ = cpu.gps_count_law(lam - h)
+        k = min(len(Pp), len(Pm), len(P))
+        assert np.abs((Pp[:k] - Pm[:k]) / (2 * h) - dP[:k]).max() < 1e-6 * max(1.0, np.abs(dP).max()), lam
+    # the render draws more points than a Poisson count below lambda ~ 0.5 (its expansion breaks down)
+    P, _ = cpu.gps_count_law(0.1)
+    assert 0.2 < float((np.arange(len(P)) * P).sum()) < 0.23
+
+
+def _gps_win_ratio(n_gaussians, k, n_samples, ss=2):
+    """Sampled over expected wins of Gaussian k (only k coloured) in the GPS render."""
+    scene, cd, *_ = _setup(n=n_gaussians)
+    sh = scene["sh_coefficients"]
+    sh[:] = 0.0
+    sh[:, 0, :] = -0.5 / 0.28209479177387814  # colour 0
+    sh[k, 0, :] = 0.5 / 0.28209479177387814   # colour 1
+    exp = cpu.expected_image(scene, cd, ss=ss, gps=True, quad=8)["image"][..., 0].sum()
+    flags = dict(aa=False, ss=ss, gps=True, hybrid=False)
+    got = 0.0
+    for f in range(n_samples):
+        got += cpu.sample_resolve(scene, cd, flags, cpu.accumulate(scene, cd, flags, 7000 + f, threads=2),
+                                  threads=2)["image"][..., 0].sum()
+    return got / n_samples / exp
+
+
+def test_gps_model_is_exact_outside_the_last_partial_warp():
+    """The render's GPS draw (accumulate_scatter.cu:104-107,126) gives the padding lanes of the scene's
+    last, partial warp the index and so the random stream of Gaussian N - 1; the cooperative points
+    those lanes draw repeat each other, so the Gaussians of that warp reach fewer pixels than N
+    independent points would. With 120 Gaussians, Gaussian 119 (about 76 points at supersampling 2,
+    some drawn by lanes 24-31) wins about 15 % less often than the model says; with 128 (no partial
+    warp) model and draw agree."""
+    assert _gps_win_ratio(120, 119, 600) < 0.93
+    assert abs(_gps_win_ratio(128, 119, 600) - 1.0) < 0.04
+    assert abs(_gps_win_ratio(120, 89, 600) - 1.0) < 0.04
+
+
+@pytest.mark.parametrize("aa,quad", [(False, 3), (True, 6)])
+def test_gps_analytic_gradient_matches_central_differences(aa, quad):
+    """The GPS expected image's gradient (hit probability through the pixel integral, the count law
+    and lambda) against central differences, with the pixel rule of the GPU (order 3) and a finer one."""
+    scene, cd, gi, ga, gd = _setup()
+    base = {k: v.copy() for k, v in scene.items()}
+    kw = dict(base=base, g_image=gi, g_alpha=ga, g_depth=gd, aa=aa, gps=True, quad=quad)
+    res = cpu.expected_image(scene, cd, grad=True, **kw)
+    rng = np.random.default_rng(2)
+    eps = 1e-3
+    worst = []
+    for k in KEYS:
+        flat = scene[k].reshape(-1)
+        for idx in rng.choice(flat.size, size=13, replace=False):
+            plus = {kk: vv.astype(np.float64).copy() for kk, vv in scene.items()}
+            minus = {kk: vv.astype(np.float64).copy() for kk, vv in scene.items()}
+            plus[k].reshape(-1)[idx] += eps
+            minus[k].reshape(-1)[idx] -= eps
+            fd = (cpu.expected_image(plus, cd, **kw)["loss"] - cpu.expected_image(minus, cd, **kw)["loss"]) / (2 * eps)
+            an = res["grad"][k].reshape(-1)[idx]
+            worst.append((abs(fd - an) / max(1e-3, abs(fd)), k, idx, fd, an))
+    worst.sort(reverse=True)
+    assert len(worst) >= 64
     assert worst[0][0] < 2e-3, worst[:5]

@@ -21,8 +21,8 @@ KEYS = ("means", "scales", "rotations", "opacities", "sh_coefficients")
 W, H = 48, 36
 
 
-def _problem(ss=1, sh_bases=16):
-    spec = sgs_scenes.SceneSpec(n=120, log_scale_mean=-2.3, log_scale_std=0.4, opacity_logit_std=1.0,
+def _problem(ss=1, sh_bases=16, n=120):
+    spec = sgs_scenes.SceneSpec(n=n, log_scale_mean=-2.3, log_scale_std=0.4, opacity_logit_std=1.0,
                                 sh_bases=sh_bases)
     scene = sgs_scenes.make_scene(spec, seed=5, morton=False)
     cam = sgs_scenes.pinhole((0.3, -0.2, -4.0), W, H, 60.0)
@@ -75,11 +75,95 @@ def test_estimator_matches_exact_gradient(ss, hybrid, store, aa, cuda_device):
         assert np.percentile(z, 99.5) < 6.0, f"{k}: z-scores {np.sort(z.ravel())[-5:]}"
 
 
+@pytest.mark.parametrize("ss,hybrid,store,aa", [(1, False, True, False), (2, True, False, False),
+                                                 (1, True, True, True)])
+def test_gps_estimator_matches_exact_gradient(ss, hybrid, store, aa, cuda_device):
+    """Gaussian point splatting (scatter and hybrid scheduling): the estimator with each fragment's alpha
+    replaced by the probability that the Gaussian puts a point into the (sub)pixel, averaged over the
+    render's own GPS samples, against the exact gradient of the GPS expected image (the count law of
+    the render's draw, the pixel integrals by an order-8 rule; the kernels use order 3 and a table of
+    the law). 128 Gaussians: the render's draw repeats the random streams of a partial last warp's
+    padding lanes, which the model does not follow (tests/test_backward_oracle_cpu.py)."""
+    scene, cam, gi, ga, gd = _problem(ss, n=128)
+    sc = {k: t.numpy() for k, t in zip(KEYS, scene.tensors())}
+    cd = dict(width=W, height=H, focal_x=cam.focal_x, focal_y=cam.focal_y, center_x=cam.center_x,
+              center_y=cam.center_y, near_plane=cam.near_plane, far_plane=cam.far_plane, w2c=cam.w2c.numpy(),
+              position=cam.position.numpy())
+    exact = cpu.expected_image(sc, cd, ss=ss, g_image=gi, g_alpha=ga, g_depth=gd, grad=True, aa=aa, gps=True,
+                               quad=8)["grad"]
+    settings = _settings(cam, ss)._replace(use_gps=True, hybrid_scheduling=hybrid, proper_antialiasing=aa)
+    gi_t = torch.tensor(gi, dtype=torch.float32, device="cuda")
+    ga_t = torch.tensor(ga, dtype=torch.float32, device="cuda")
+    gd_t = torch.tensor(gd, dtype=torch.float32, device="cuda")
+    batches, per_batch = 16, 512
+    est = {k: [] for k in KEYS}
+    for bi in range(batches):
+        params = [t.cuda().requires_grad_(True) for t in scene.tensors()]
+        image, depth, alpha = render_samples(*params, settings, n_samples=per_batch, first_frame=7000 + bi * per_batch,
+                                             store_winners=store)
+        loss = (image * gi_t).sum() + (alpha * ga_t).sum() + (depth * gd_t).sum()
+        loss.backward()
+        for k, p in zip(KEYS, params):
+            est[k].append(p.grad.detach().cpu().numpy().astype(np.float64))
+    for k in KEYS:
+        e = np.stack(est[k])
+        mean = e.mean(0)
+        se = e.std(0, ddof=1) / np.sqrt(batches)
+        ex = exact[k]
+        rel = np.linalg.norm(mean - ex) / np.linalg.norm(ex)
+        z = np.abs(mean - ex) / np.maximum(se, 1e-6 * np.abs(ex).max())
+        assert rel < 0.06, f"{k}: relative L2 error {rel:.4f}"
+        assert np.percentile(z, 99.5) < 6.0, f"{k}: z-scores {np.sort(z.ravel())[-5:]}"
+
+
+def test_gps_count_law_table_matches_the_oracle(cuda_device):
+    """The table the GPS backward builds per call (sgs_gps_count_law: P(N = n) and dP/dlambda of the
+    render's point count, 1025 rows over log2(lambda) in [-10, 3], N >= 31 in the last term) against
+    the oracle's law at every 16th row."""
+    import ctypes
+
+    from StochasticGSCudaBackend import _abi
+
+    lib = _abi.load()
+    n_bytes = lib.sgs_gps_count_law_size()
+    assert n_bytes == 1025 * 32 * 8
+    buf = torch.empty(n_bytes // 4, dtype=torch.float32, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.sgs_gps_count_law(ctypes.c_void_p(buf.data_ptr()), stream) == _abi.SGS_OK
+    table = buf.view(1025, 32, 2).cpu().numpy().astype(np.float64)
+    for r in list(range(0, 1025, 16)) + [1024]:
+        P, dP = cpu.gps_count_law(2.0 ** (-10.0 + 13.0 * r / 1024.0))
+        want, dwant = np.zeros(32), np.zeros(32)
+        k = min(31, len(P))
+        want[:k], dwant[:k] = P[:k], dP[:k]
+        want[31], dwant[31] = 1.0 - want[:31].sum(), -dwant[:31].sum()
+        assert np.abs(table[r, :, 0] - want).max() < 2e-6, r
+        assert np.abs(table[r, :, 1] - dwant).max() < 1e-4 * max(1.0, np.abs(dwant).max()), r
+
+
 def test_backward_rejects_unsupported_modes(cuda_device):
+    """Spatial reuse is not differentiated; GPS gradients come from the fused walk only (the per-sample
+    sgs_backward_accumulate rejects GPS settings)."""
+    import ctypes
+
+    from StochasticGSCudaBackend import _abi
+    from StochasticGSCudaBackend.autograd import _structs
+
     scene, cam, *_ = _problem()
     params = [t.cuda().requires_grad_(True) for t in scene.tensors()]
-    with pytest.raises(RuntimeError, match="stochastic transparency"):
-        render_samples(*params, _settings(cam, 1)._replace(use_gps=True), n_samples=2)
+    with pytest.raises(RuntimeError, match="spatial reuse"):
+        render_samples(*params, _settings(cam, 1)._replace(spatial_reuse=True), n_samples=2)
+    lib = _abi.load()
+    tensors = tuple(t.detach().contiguous() for t in params)
+    g, c, s = _structs(*tensors, _settings(cam, 1)._replace(use_gps=True))
+    bw = torch.empty(lib.sgs_backward_workspace_size(tensors[0].shape[0]) // 4 + 4, device="cuda")
+    grad = torch.zeros((H, W, 3), device="cuda")
+    ws = torch.zeros(1 << 20, dtype=torch.uint8, device="cuda")
+    st = lib.sgs_backward_accumulate(ctypes.byref(g), ctypes.byref(c), ctypes.byref(s), ctypes.c_void_p(ws.data_ptr()),
+                                     ctypes.c_void_p(grad.data_ptr()), None, None, ctypes.c_float(1.0), 1,
+                                     ctypes.c_void_p(bw.data_ptr()), None)
+    assert st == _abi.SGS_ERROR_INVALID_ARGUMENT
+    assert "fused walk" in _abi.last_error(lib)
 
 
 def _big_problem(ss=1):
