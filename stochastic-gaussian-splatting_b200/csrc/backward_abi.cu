@@ -3,6 +3,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "../../include/sgs_b200.h"
+#include "sgs_backward_gps.h"
 #include "sgs_internal.h"
 
 namespace {
@@ -15,6 +16,7 @@ struct BackwardSetup {
     BackwardParams p;
     sgs_workspace_layout layout;
     bool gps;
+    float2* gps_law;  // GPS: the count-law table in the sample scratch
 };
 
 int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, BackwardSetup& out) {
@@ -58,8 +60,8 @@ int setup(const sgs_gaussians* g, const sgs_camera* c, const sgs_settings* s, Ba
     p.width = c->width;
     p.ss = ss;
     p.n_fb = c->width * ss * c->height * ss;
-    p.gps_law = nullptr;
     out.gps = s->use_gps != 0;
+    out.gps_law = nullptr;
     return SGS_OK;
 }
 
@@ -68,8 +70,8 @@ constexpr uint32_t kMaxFusedSamples = 1024;
 size_t align256(const size_t v) { return (v + 255) & ~size_t(255); }
 
 // Interleaved per-pixel sample table of the fused backward: keys, then terms, the per-pixel largest
-// key, and for GPS the count-law table.
-void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples, const bool gps) {
+// key, and for GPS the count-law table (returned; null without GPS).
+float2* set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples, const bool gps) {
     p.n_samples = n_samples;
     p.pix_keys = static_cast<unsigned long long*>(scratch);
     const size_t keys = align256(sizeof(unsigned long long) * p.n_fb * static_cast<size_t>(n_samples));
@@ -77,7 +79,12 @@ void set_sample_table(BackwardParams& p, void* scratch, const uint32_t n_samples
     const size_t max_keys = align256(sizeof(unsigned long long) * p.n_fb);
     p.pix_terms = reinterpret_cast<float*>(static_cast<char*>(scratch) + keys);
     p.pix_max_key = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + keys + terms);
-    p.gps_law = gps ? reinterpret_cast<float2*>(static_cast<char*>(scratch) + keys + terms + max_keys) : nullptr;
+    return gps ? reinterpret_cast<float2*>(static_cast<char*>(scratch) + keys + terms + max_keys) : nullptr;
+}
+
+cudaError_t launch_walk(const BackwardSetup& S, cudaStream_t stream) {
+    return S.gps ? launch_backward_fragments_samples_gps(S.p, S.gps_law, stream)
+                 : launch_backward_fragments_samples(S.p, stream);
 }
 
 // Entries of the large-Gaussian queue of the fused walk (at most 2^18).
@@ -196,7 +203,7 @@ int sgs_backward_sample_terms(const sgs_gaussians* gaussians, const sgs_camera* 
     p.grad_alpha = grad_alpha;
     p.grad_depth = grad_depth;
     p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
-    set_sample_table(p, scratch, n_samples, S.gps);
+    S.gps_law = set_sample_table(p, scratch, n_samples, S.gps);
     p.sample = sample;
     const cudaError_t err = launch_backward_sample_terms(p, static_cast<cudaStream_t>(stream_ptr));
     if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
@@ -222,7 +229,7 @@ int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_ca
     p.grad_alpha = grad_alpha;
     p.grad_depth = grad_depth;
     p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
-    set_sample_table(p, scratch, n_samples, S.gps);
+    S.gps_law = set_sample_table(p, scratch, n_samples, S.gps);
     set_backward_buffers(p, backward_workspace);
     cudaError_t err = cudaSuccess;
     if (first) {
@@ -235,7 +242,7 @@ int sgs_backward_accumulate_samples(const sgs_gaussians* gaussians, const sgs_ca
         err = cudaGetDevice(&device);
         if (err == cudaSuccess) err = cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, device);
     }
-    if (err == cudaSuccess) err = launch_backward_fragments_samples(p, stream);
+    if (err == cudaSuccess) err = launch_walk(S, stream);
     if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
     return SGS_OK;
 }
@@ -262,7 +269,7 @@ int sgs_backward_accumulate_framebuffers(const sgs_gaussians* gaussians, const s
     p.grad_alpha = grad_alpha;
     p.grad_depth = grad_depth;
     p.grad_scale = weight / static_cast<float>(p.ss * p.ss);
-    set_sample_table(p, scratch, n_samples, S.gps);
+    S.gps_law = set_sample_table(p, scratch, n_samples, S.gps);
     set_backward_buffers(p, backward_workspace);
     cudaError_t err = cudaSuccess;
     if (first) err = cudaMemsetAsync(p.accum, 0, kAccumFloats * p.n * sizeof(float), stream);
@@ -274,7 +281,7 @@ int sgs_backward_accumulate_framebuffers(const sgs_gaussians* gaussians, const s
         err = cudaGetDevice(&device);
         if (err == cudaSuccess) err = cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, device);
     }
-    if (err == cudaSuccess) err = launch_backward_fragments_samples(p, stream);
+    if (err == cudaSuccess) err = launch_walk(S, stream);
     if (err != cudaSuccess) return record_error(SGS_ERROR_CUDA, "backward: %s", cudaGetErrorString(err));
     return SGS_OK;
 }

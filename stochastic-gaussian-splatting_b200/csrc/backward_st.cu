@@ -17,6 +17,7 @@
 // come from re-rendering the sample (same frame index) or from its stored framebuffer.
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "sgs_backward_gps.h"
 #include "sgs_internal.h"
 #include "sgs_rows.cuh"
 
@@ -44,7 +45,8 @@ constexpr int kAccum = 10;               // op, conic x/y/z, mean2d x/y, depth, 
 // independently of the other Gaussians: the stochastic-transparency estimator holds with alpha
 // replaced by h. Lambda_p and its derivatives come from a 3 x 3 Gauss-Legendre rule over the pixel.
 // P(N = n) and dP/dlambda come from a table over log2(lambda) in [-10, 3] (32 terms, the rest of
-// the law folded into the last), built per call by gps_count_law_kernel; from lambda = 8 up the
+// the law folded into the last), built per call by gps_count_law_kernel (sgs_backward_gps.h) in the
+// caller's scratch; from lambda = 8 up the
 // count is taken as Poisson (Q = exp(-Lambda_p)), which the draw matches there to within 3e-4.
 constexpr int kLawRows = 1025;
 constexpr int kLawTerms = 32;
@@ -456,9 +458,9 @@ static_assert(sizeof(WalkEntry) == 128, "the backward workspace reserves 128 byt
 // (constants gc) instead of alpha.
 template <bool kGps>
 __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, const WalkGaussian& q,
-                                                   const GpsConstants& gc, const bool valid, const uint32_t y,
-                                                   FragAccum& acc, const uint32_t seg = 0,
-                                                   const uint32_t log_segs = 0) {
+                                                   const GpsConstants& gc, const float2* __restrict__ law,
+                                                   const bool valid, const uint32_t y, FragAccum& acc,
+                                                   const uint32_t seg = 0, const uint32_t log_segs = 0) {
     uint32_t xs = 0, len = 0;
     float dy = 0.0f;
     if (valid) {
@@ -527,7 +529,7 @@ __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, cons
                     // h = 1 - Q: dL/dh from the samples, then through Q's partial derivatives
                     const GpsFragment f = gps_fragment(q.cx, q.cy, q.cz, q.opacity,
                                                        make_float3(q.conic_x, q.conic_y, q.conic_z), gc, dx, dy,
-                                                       b.gps_law);
+                                                       law);
                     const float inv = 1.0f / fmaxf(f.Q, 1e-12f);
                     const float dH = static_cast<float>(ge) * gck - inv * behind + inv * ga * static_cast<float>(none);
                     acc.v[0] -= dH * f.dQ_op;
@@ -561,7 +563,7 @@ __device__ __forceinline__ void walk_row_gradients(const BackwardParams& b, cons
 // One thread per Gaussian: the rows of a warp's 32 Gaussians are laid end to end, 32 per step, and
 // each lane walks one row; the row sums go to per-Gaussian accumulators in shared memory.
 template <bool kGps>
-__global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const BackwardParams b) {
+__global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const BackwardParams b, const float2* __restrict__ law) {
     __shared__ WalkGaussian s_g[kWarpsPerBlock][32];
     __shared__ GpsConstants s_c[kGps ? kWarpsPerBlock : 1][32];
     __shared__ float s_acc[kWarpsPerBlock][32][kAccum];
@@ -648,7 +650,7 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
         FragAccum acc;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
-        walk_row_gradients<kGps>(b, rq, rc, valid, rq.y_min + (r - rq.row_first), acc);
+        walk_row_gradients<kGps>(b, rq, rc, law, valid, rq.y_min + (r - rq.row_first), acc);
         if (valid) {
 #pragma unroll
             for (int i = 0; i < kAccum; ++i)
@@ -669,7 +671,8 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_kernel(const Backwar
 // (R rows, each split into 32 / R lane segments), sums the lanes' gradients and adds them to the
 // Gaussian's accumulators.
 template <bool kGps>
-__global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const BackwardParams b) {
+__global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const BackwardParams b,
+                                                                         const float2* __restrict__ law) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long packed = b.bw_queue->packed;
     const uint32_t n_entries =
@@ -705,7 +708,7 @@ __global__ void __launch_bounds__(kBlock) fragments_samples_queue_kernel(const B
         FragAccum acc;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) acc.v[i] = 0.0f;
-        walk_row_gradients<kGps>(b, q, gc, r < m.y, q.y_min + r, acc, lane >> log_rows, 5u - log_rows);
+        walk_row_gradients<kGps>(b, q, gc, law, r < m.y, q.y_min + r, acc, lane >> log_rows, 5u - log_rows);
         float* out = b.accum + static_cast<size_t>(b.bw_index[lo]) * kAccum;
 #pragma unroll
         for (int i = 0; i < kAccum; ++i) {
@@ -928,14 +931,19 @@ cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStrea
     if (p.n == 0) return cudaSuccess;
     const unsigned grid = (p.n + kBlock - 1) / kBlock;
     const unsigned queue_grid = static_cast<unsigned>(max(p.num_sms, 1)) * kQueueBlocksPerSM;
-    if (p.gps_law != nullptr) {
-        gps_count_law_kernel<<<kLawRows, 32, 0, stream>>>(p.gps_law);
-        fragments_samples_kernel<true><<<grid, kBlock, 0, stream>>>(p);
-        fragments_samples_queue_kernel<true><<<queue_grid, kBlock, 0, stream>>>(p);
-    } else {
-        fragments_samples_kernel<false><<<grid, kBlock, 0, stream>>>(p);
-        fragments_samples_queue_kernel<false><<<queue_grid, kBlock, 0, stream>>>(p);
-    }
+    fragments_samples_kernel<false><<<grid, kBlock, 0, stream>>>(p, nullptr);
+    fragments_samples_queue_kernel<false><<<queue_grid, kBlock, 0, stream>>>(p, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_fragments_samples_gps(const BackwardParams& p, float2* law, cudaStream_t stream) {
+    if (p.n == 0) return cudaSuccess;
+    if (law == nullptr) return cudaErrorInvalidValue;
+    const unsigned grid = (p.n + kBlock - 1) / kBlock;
+    const unsigned queue_grid = static_cast<unsigned>(max(p.num_sms, 1)) * kQueueBlocksPerSM;
+    gps_count_law_kernel<<<kLawRows, 32, 0, stream>>>(law);
+    fragments_samples_kernel<true><<<grid, kBlock, 0, stream>>>(p, law);
+    fragments_samples_queue_kernel<true><<<queue_grid, kBlock, 0, stream>>>(p, law);
     return cudaGetLastError();
 }
 

@@ -209,9 +209,6 @@ struct BackwardParams {
     uint32_t n_samples;                      // S
     uint32_t sample;                         // the sample whose terms sample_terms writes
     uint32_t n_fb;                           // framebuffer pixels
-    // Gaussian point splatting: the table of the point count's law (gps_count_law_bytes(), built
-    // by launch_backward_fragments_samples before the walk), or null for stochastic transparency
-    float2* gps_law;
 };
 
 cudaError_t launch_backward_colors(const BackwardParams& p, cudaStream_t stream);
@@ -220,9 +217,6 @@ cudaError_t launch_backward_projection(const BackwardParams& p, cudaStream_t str
 cudaError_t launch_backward_sample_terms(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_framebuffer_terms(const BackwardParams& p, cudaStream_t stream);
 cudaError_t launch_backward_fragments_samples(const BackwardParams& p, cudaStream_t stream);
-// Bytes of the GPS count-law table and its construction alone (the fused walk builds it itself).
-size_t gps_count_law_bytes();
-cudaError_t launch_gps_count_law(float2* law, cudaStream_t stream);
 
 // Sets the calling thread's sgs_last_error() message (printf format) and returns `status`.
 int record_error(int status, const char* fmt, ...);
