@@ -185,3 +185,21 @@ def test_no_alloc_scratch_bounds_hold():
     assert size(285_000, 1, 1) <= limit < size(295_000, 1, 1)
     assert size(6_000_000, 1, 1, max_binned=285_000) <= limit
     assert size(1_000_000, 1, 1) > limit
+
+
+def test_gps_backward_scratch_holds_the_count_law_table():
+    """The GPS backward's table of the point count's law (1025 rows x 32 float pairs) sits in the
+    fused walk's scratch after the per-pixel sample table: GPS settings add exactly its size."""
+    lib = _abi.load()
+    table = lib.sgs_gps_count_law_size()
+    assert table == 1025 * 32 * 8 and table % 256 == 0
+    for ss, n_samples in ((1, 1), (2, 8), (3, 5)):
+        _, c, s_st = _args(width=96, height=64, ss=ss)
+        _, _, s_gps = _args(width=96, height=64, ss=ss, gps=1)
+        _, _, s_hyb = _args(width=96, height=64, ss=ss, gps=1, hybrid=1)
+        st = lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s_st), n_samples)
+        n_fb = 96 * 64 * ss * ss
+        align = lambda v: (v + 255) // 256 * 256  # noqa: E731
+        assert st == align(8 * n_fb * n_samples) + align(4 * n_fb * n_samples) + align(8 * n_fb)
+        assert lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s_gps), n_samples) == st + table
+        assert lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s_hyb), n_samples) == st + table
