@@ -151,21 +151,23 @@ def _f64(a) -> np.ndarray:
 
 
 def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None, g_image=None, g_alpha=None,
-                   g_depth=None, grad: bool = False, aa: bool = False, gps: bool = False, quad: int = 8) -> dict:
+                   g_depth=None, grad: bool = False, aa: bool = False, gps: bool = False, quad: int = 8,
+                   max_fragments: int = 0) -> dict:
     """Expected image of one stochastic-transparency sample (double precision) and, with `grad`, the
     gradient of sum(g_image * image + g_alpha * alpha + g_depth * depth) w.r.t. every parameter.
     The fragment support and key order are frozen at `base` (single precision; default: `scene`).
     `aa`: proper antialiasing (smaller dilation, opacity scaled by sqrt(det / det dilated)).
     `gps`: Gaussian point splatting instead, each fragment's alpha replaced by the probability that
     the Gaussian puts a point into the (sub)pixel, its pixel integrals by an order-`quad`
-    Gauss-Legendre rule per axis."""
+    Gauss-Legendre rule per axis, and the point count capped at `max_fragments` as the render caps it
+    (0: the render's default cap, < 0: no cap)."""
     l = lib()
     P, u, d, i = _P, ctypes.c_uint32, ctypes.c_double, ctypes.c_int
     args = [P, P, P, P, P, u, u, P, P, u, u, d, d, d, d, d, d, i, i, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P]
     if not hasattr(l.oracle_expected_image, "_typed"):
         l.oracle_expected_image.argtypes = args
         l.oracle_expected_image._typed = True
-        l.oracle_expected_image_gps.argtypes = args + [i]
+        l.oracle_expected_image_gps.argtypes = args + [i, i]
     base = scene if base is None else base
     m, s, r, o, sh = (_f64(scene[k]) for k in ("means", "scales", "rotations", "opacities", "sh_coefficients"))
     bm, bs, br, bo = (_f32(base[k]) for k in ("means", "scales", "rotations", "opacities"))
@@ -189,7 +191,7 @@ def expected_image(scene: dict, cam: dict, ss: int = 1, base: dict | None = None
             ctypes.byref(loss),
             *(_p(out[k]) if grad else None for k in ("means", "scales", "rotations", "opacities", "sh_coefficients")))
     if gps:
-        l.oracle_expected_image_gps(*call, int(quad))
+        l.oracle_expected_image_gps(*call, int(quad), int(max_fragments))
     else:
         l.oracle_expected_image(*call)
     return {"image": image, "alpha": alpha, "depth": depth, "loss": loss.value, "grad": out if grad else None}

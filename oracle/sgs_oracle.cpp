@@ -1194,7 +1194,9 @@ FragP st_fragment(const ProjD& p, const double px, const double py) {
 
 // Per-Gaussian constants of the GPS hit probability: lambda, its derivatives in (op, conic x/y/z)
 // and the law of the count (above kPoissonLambda the count is taken as Poisson, which the
-// Cornish-Fisher draw matches to about 1e-5 there).
+// Cornish-Fisher draw matches to about 1e-5 there). With a point cap c (the render draws
+// min(N, c) points, accumulate_scatter.cu:129-131), the law is truncated at c and P(N >= c) folded
+// into the term of c: Q = sum_{n < c} P(N = n) Z^n + P(N >= c) Z^c.
 struct GpsLaw {
     double lam, d_lam[4];
     bool poisson;
@@ -1202,7 +1204,26 @@ struct GpsLaw {
 };
 constexpr double kOraclePoissonLambda = 32.0;
 
-GpsLaw gps_law(const ProjD& p) {
+// Poisson law of n < cap with the rest folded into the term of cap, and its lambda-derivative
+// (d pmf(n) / d lambda = pmf(n - 1) - pmf(n); the folded rest's is pmf(cap - 1)).
+CountLaw poisson_law_capped(const double lam, const uint32_t cap) {
+    CountLaw law;
+    law.P.resize(cap + 1);
+    law.dP.resize(cap + 1);
+    double prev = 0.0, sum = 0.0;
+    for (uint32_t n = 0; n < cap; ++n) {
+        const double pmf = std::exp(n * std::log(lam) - lam - std::lgamma(n + 1.0));
+        law.P[n] = pmf;
+        law.dP[n] = prev - pmf;
+        sum += pmf;
+        prev = pmf;
+    }
+    law.P[cap] = std::max(1.0 - sum, 0.0);
+    law.dP[cap] = prev;
+    return law;
+}
+
+GpsLaw gps_law(const ProjD& p, const uint32_t cap) {
     GpsLaw g;
     const double two_pi = 2.0 * 3.14159265358979323846;
     const double sd = std::sqrt(p.det);
@@ -1213,7 +1234,23 @@ GpsLaw gps_law(const ProjD& p) {
     g.d_lam[2] = g.lam * p.conic[1] / D;
     g.d_lam[3] = g.lam * (-0.5) * p.conic[0] / D;
     g.poisson = g.lam >= kOraclePoissonLambda;
-    if (!g.poisson) g.law = cf_count_law(g.lam);
+    if (!g.poisson) {
+        g.law = cf_count_law(g.lam);
+        if (cap > 0 && cap < g.law.P.size()) {
+            double rest = 0.0, d_rest = 0.0;
+            for (size_t n = cap; n < g.law.P.size(); ++n) {
+                rest += g.law.P[n];
+                d_rest += g.law.dP[n];
+            }
+            g.law.P.resize(cap + 1);
+            g.law.dP.resize(cap + 1);
+            g.law.P[cap] = rest;
+            g.law.dP[cap] = d_rest;
+        }
+    } else if (cap > 0 && g.lam + 12.0 * std::sqrt(g.lam) >= cap) {
+        g.poisson = false;  // the cap binds: the capped Poisson law through the general form
+        g.law = poisson_law_capped(g.lam, cap);
+    }
     return g;
 }
 
@@ -1295,7 +1332,8 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
 // The same for Gaussian point splatting: each fragment's alpha is replaced by the probability that
 // the Gaussian puts a point into the (sub)pixel (see gps_fragment), with the pixel integrals taken
 // by an order-`quad` Gauss-Legendre rule per axis. The support is the pixels whose centre passes the
-// power test at the base point, as in the render (scatter_utils.cuh:116-129).
+// power test at the base point, as in the render (scatter_utils.cuh:116-129). `max_fragments`: the
+// point cap (0: the render's default, width x height / (2 ss^2) framebuffer pixels; < 0: none).
 int oracle_expected_image_gps(const double* means, const double* scales, const double* rotations,
                               const double* opacities, const double* sh, uint32_t n, uint32_t bases, const double* w2c,
                               const double* cam_pos, uint32_t width, uint32_t height, double fx, double fy, double cx,
@@ -1304,7 +1342,7 @@ int oracle_expected_image_gps(const double* means, const double* scales, const d
                               const float* base_opacities, const double* g_image, const double* g_alpha,
                               const double* g_depth, double* image, double* alpha, double* depth, double* loss,
                               double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
-                              double* d_sh, int quad);
+                              double* d_sh, int quad, int max_fragments);
 
 }  // extern "C"
 
@@ -1317,7 +1355,7 @@ int expected_image_impl(const double* means, const double* scales, const double*
                         const float* base_rotations, const float* base_opacities, const double* g_image,
                         const double* g_alpha, const double* g_depth, double* image, double* alpha, double* depth,
                         double* loss, double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
-                        double* d_sh, const bool gps, const int quad) {
+                        double* d_sh, const bool gps, const int quad, const int cap_arg) {
     const uint32_t ss = ss_raw < 1 ? 1u : static_cast<uint32_t>(ss_raw);
     float w2cf[12];
     for (int i = 0; i < 12; ++i) w2cf[i] = static_cast<float>(w2c[i]);
@@ -1354,7 +1392,12 @@ int expected_image_impl(const double* means, const double* scales, const double*
                           bases, w2c, cam_pos, dfx, dfy, dcx, dcy, static_cast<double>(fbw), static_cast<double>(fbh), dil,
                           aa != 0);
     std::vector<GpsLaw> laws(gps ? n : 0);
-    for (uint32_t g = 0; g < n && gps; ++g) laws[g] = gps_law(pd[g]);
+    // the render's point cap: width x height / (2 ss^2) framebuffer pixels unless given; < 0: none
+    const uint32_t cap = cap_arg < 0 ? 0u
+                         : cap_arg > 0 ? static_cast<uint32_t>(cap_arg)
+                                       : static_cast<uint32_t>(std::nearbyint(static_cast<float>(fbw) * static_cast<float>(fbh) /
+                                                                              (2.0f * ss * ss)));
+    for (uint32_t g = 0; g < n && gps; ++g) laws[g] = gps_law(pd[g], cap);
     std::vector<double> qx, qw;
     if (gps) gauss_legendre01(std::max(quad, 1), qx, qw);
     const bool grad = d_means != nullptr;
@@ -1447,7 +1490,7 @@ int oracle_expected_image(const double* means, const double* scales, const doubl
     return expected_image_impl(means, scales, rotations, opacities, sh, n, bases, w2c, cam_pos, width, height, fx, fy,
                                cx, cy, near_plane, far_plane, ss_raw, aa, base_means, base_scales, base_rotations,
                                base_opacities, g_image, g_alpha, g_depth, image, alpha, depth, loss, d_means, d_scales,
-                               d_rotations, d_opacities, d_sh, false, 0);
+                               d_rotations, d_opacities, d_sh, false, 0, 0);
 }
 
 int oracle_expected_image_gps(const double* means, const double* scales, const double* rotations,
@@ -1458,11 +1501,11 @@ int oracle_expected_image_gps(const double* means, const double* scales, const d
                               const float* base_opacities, const double* g_image, const double* g_alpha,
                               const double* g_depth, double* image, double* alpha, double* depth, double* loss,
                               double* d_means, double* d_scales, double* d_rotations, double* d_opacities,
-                              double* d_sh, int quad) {
+                              double* d_sh, int quad, int max_fragments) {
     return expected_image_impl(means, scales, rotations, opacities, sh, n, bases, w2c, cam_pos, width, height, fx, fy,
                                cx, cy, near_plane, far_plane, ss_raw, aa, base_means, base_scales, base_rotations,
                                base_opacities, g_image, g_alpha, g_depth, image, alpha, depth, loss, d_means, d_scales,
-                               d_rotations, d_opacities, d_sh, true, quad);
+                               d_rotations, d_opacities, d_sh, true, quad, max_fragments);
 }
 
 }  // extern "C"

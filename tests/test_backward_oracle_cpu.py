@@ -180,30 +180,60 @@ def test_gps_analytic_gradient_matches_central_differences(aa, quad):
     assert worst[0][0] < 2e-3, worst[:5]
 
 
-def test_gps_model_covers_binned_gaussians_but_not_the_point_cap():
-    """Hybrid scheduling draws the points of Gaussians with more than 512 of them from per-point seeds
-    in the work queue (accumulate_hybrid_gps.cu:126-181): with the per-Gaussian point cap lifted, the
-    mean alpha of the render matches the model. The cap itself (max_fragments, by default width x
-    height / 2 image pixels: 3456 here, which two of these Gaussians exceed) is not in the model: the
-    capped Gaussians reach fewer pixels and the mean alpha falls below it."""
-    W, H, ss = 96, 72, 2
+def _capped_scene():
+    """96x72 at supersampling 2, 64 Gaussians: 16 with more than 512 points (binned by hybrid
+    scheduling), two of which (44 and 62, lambda about 3150 and 4430) reach the render's default
+    point cap of width x height / 2 image pixels = 3456."""
+    W, H = 96, 72
     spec = sgs_scenes.SceneSpec(n=64, log_scale_mean=-1.2, log_scale_std=0.4, opacity_logit_std=1.0)
     scene = {k: t.numpy() for k, t in zip(KEYS, sgs_scenes.make_scene(spec, seed=7, morton=False).tensors())}
     cam = sgs_scenes.pinhole((0.3, -0.2, -4.0), W, H, 60.0)
     cd = dict(width=W, height=H, focal_x=cam.focal_x, focal_y=cam.focal_y, center_x=cam.center_x,
               center_y=cam.center_y, near_plane=cam.near_plane, far_plane=cam.far_plane, w2c=cam.w2c.numpy(),
               position=cam.position.numpy())
-    want = cpu.expected_image(scene, cd, ss=ss, gps=True, quad=8)["alpha"]
+    return scene, cd
+
+
+def test_gps_model_covers_binned_gaussians_and_the_point_cap():
+    """Hybrid scheduling draws the points of Gaussians with more than 512 of them from per-point seeds
+    in the work queue (accumulate_hybrid_gps.cu:126-181), and the render draws at most max_fragments
+    points per Gaussian (accumulate_scatter.cu:129-131). The mean alpha of the render matches the
+    model with the cap (the law truncated at the cap) and, with the cap lifted, the model without it;
+    the cap moves the model by -0.0064 on this scene (the kernels' model leaves the cap out)."""
+    scene, cd = _capped_scene()
+    ss = 2
+    uncapped = cpu.expected_image(scene, cd, ss=ss, gps=True, quad=8, max_fragments=-1)["alpha"]
+    capped = cpu.expected_image(scene, cd, ss=ss, gps=True, quad=8)["alpha"]
     flags = dict(aa=False, ss=ss, gps=True, hybrid=True)
 
     def mean_alpha(max_fragments, n=300):
-        acc = np.zeros_like(want)
+        acc = np.zeros_like(capped)
         for f in range(n):
             fb = cpu.accumulate(scene, cd, flags, 500 + f, max_fragments=max_fragments, threads=2)
             acc += cpu.sample_resolve(scene, cd, flags, fb, threads=2)["alpha"]
         return acc / n
 
-    uncapped = float((mean_alpha(1_000_000) - want).mean())
-    capped = float((mean_alpha(0) - want).mean())
-    assert abs(uncapped) < 0.0012, uncapped
-    assert capped < -0.004, capped
+    assert float((capped - uncapped).mean()) < -0.004
+    assert abs(float((mean_alpha(1_000_000) - uncapped).mean())) < 0.0012
+    assert abs(float((mean_alpha(0) - capped).mean())) < 0.0012
+
+
+def test_gps_capped_gradient_matches_central_differences():
+    """The gradient through the capped count law (Poisson terms below the cap, the rest folded into the
+    cap's term) of the two capped Gaussians' opacity, scale and mean."""
+    scene, cd = _capped_scene()
+    rng = np.random.default_rng(0)
+    gi = rng.normal(size=(72, 96, 3))
+    ga = rng.normal(size=(72, 96, 1))
+    kw = dict(ss=2, base={k: v.copy() for k, v in scene.items()}, g_image=gi, g_alpha=ga, gps=True, quad=3)
+    res = cpu.expected_image(scene, cd, grad=True, **kw)
+    eps = 1e-3
+    for g in (44, 62):
+        for k, idx in (("opacities", (g,)), ("scales", (g, 0)), ("means", (g, 1))):
+            plus = {kk: vv.astype(np.float64).copy() for kk, vv in scene.items()}
+            minus = {kk: vv.astype(np.float64).copy() for kk, vv in scene.items()}
+            plus[k][idx] += eps
+            minus[k][idx] -= eps
+            fd = (cpu.expected_image(plus, cd, **kw)["loss"] - cpu.expected_image(minus, cd, **kw)["loss"]) / (2 * eps)
+            an = res["grad"][k][idx]
+            assert abs(fd - an) <= 1e-4 * max(1e-3, abs(fd)), (g, k, fd, an)
