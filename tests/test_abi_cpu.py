@@ -203,3 +203,23 @@ def test_gps_backward_scratch_holds_the_count_law_table():
         assert st == align(8 * n_fb * n_samples) + align(4 * n_fb * n_samples) + align(8 * n_fb)
         assert lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s_gps), n_samples) == st + table
         assert lib.sgs_backward_samples_scratch_size(ctypes.byref(c), ctypes.byref(s_hyb), n_samples) == st + table
+
+
+def test_count_law_and_autograd_reject_bad_input_before_any_launch():
+    """sgs_gps_count_law wants an 8-byte aligned buffer; render_samples refuses spatial reuse (its
+    samples mix neighbours' winners through the k-buffer) before touching the device."""
+    import torch
+
+    from StochasticGSCudaBackend import Settings
+    from StochasticGSCudaBackend.autograd import render_samples
+
+    lib = _abi.load()
+    assert lib.sgs_gps_count_law(None, None) == _abi.SGS_ERROR_INVALID_ARGUMENT
+    assert lib.sgs_gps_count_law(ctypes.c_void_p(0x10004), None) == _abi.SGS_ERROR_INVALID_ARGUMENT
+    assert "8-byte aligned" in _abi.last_error(lib)
+    params = [torch.zeros((4, 3)), torch.zeros((4, 3)), torch.zeros((4, 4)), torch.zeros((4,)),
+              torch.zeros((4, 16, 3))]
+    settings = Settings(torch.eye(4), torch.zeros(3), 32, 24, 30.0, 30.0, 16.0, 12.0, 0.2, 100.0, False, 1, False,
+                        False, True)
+    with pytest.raises(RuntimeError, match="spatial reuse"):
+        render_samples(*params, settings, n_samples=2, first_frame=0)
